@@ -1,0 +1,150 @@
+/*
+ * nest_b200 -- C ABI of the B200-native nest hot path.
+ *
+ * Plain C: pointers, sizes and status codes only.  Device memory is owned by
+ * the library unless an entry point says otherwise; host buffers are owned
+ * by the caller.  No entry point throws: failures return a status (or, for
+ * the nest-compatible void/pointer functions, are recorded and readable
+ * through nest_last_error() / euler1d_gpu_status()).
+ *
+ * Paths of the form file:line refer to the nest source tree.
+ */
+#ifndef NEST_B200_H
+#define NEST_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status and errors                                                        */
+/* ------------------------------------------------------------------------ */
+
+/* nest's C ABI reports CUDA failures by throwing std::runtime_error through
+ * extern "C" (src/backend_cuda/euler1d_solver.cu:24-29); here every failure
+ * is a status code. */
+typedef enum nest_status {
+    NEST_OK = 0,
+    NEST_ERR_INVALID = 1,     /* bad argument or handle */
+    NEST_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    NEST_ERR_OOM = 3,         /* device allocation failed */
+    NEST_ERR_NUMERIC = 4,     /* non-finite wave speed (state blew up) */
+    NEST_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+    NEST_ERR_UNSUPPORTED = 6  /* valid request this build does not implement */
+} nest_status;
+
+/* Message of the last failing call on the calling thread ("" if none). */
+const char* nest_last_error(void);
+/* ABI version: major * 10000 + minor * 100 + patch. */
+int nest_version(void);
+
+enum { NEST_BC_PERIODIC = 0, NEST_BC_OUTFLOW = 1 };
+enum { NEST_F64 = 0, NEST_F32 = 1 };
+/* Host/device array layouts for upload/download.
+ *   EXTENDED: SoA over the extended space, halos included.  1D: [var][n+2h]
+ *             (euler1d_solver.hpp:38-40).  2D: [var][nx+4][ny+4] with the y
+ *             index fastest (include/nest/core.hpp:206-215).
+ *   INTERIOR: SoA over the interior only: 1D [var][n], 2D [var][nx][ny]. */
+enum { NEST_LAYOUT_EXTENDED = 0, NEST_LAYOUT_INTERIOR = 1 };
+enum {
+    NEST_FLAG_TOTALS = 1,       /* keep FP64 conserved totals each step (2D) */
+    NEST_FLAG_REPAIR = 2,       /* FP32 form: FP64 positivity repair near vacuum */
+    NEST_FLAG_NO_RESIDENT = 4   /* 1D: never use the single-CTA resident solver */
+};
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in: nest's 1D CUDA solver ABI                                       */
+/* Same names, signatures, SoA-with-halo host layout and periodic boundary  */
+/* as src/backend_cuda/euler1d_solver.hpp:16-87.                            */
+/* ------------------------------------------------------------------------ */
+
+typedef struct euler1d_gpu_t euler1d_gpu_t;
+
+/* euler1d_solver.hpp:27.  NULL on failure (see nest_last_error()). */
+euler1d_gpu_t* euler1d_gpu_create(int n_interior, int n_halo, double dx, double gamma);
+/* euler1d_solver.hpp:32. */
+void euler1d_gpu_destroy(euler1d_gpu_t* solver);
+/* euler1d_solver.hpp:41: h_data is SoA [var * n_total + i], n_total = n_interior + 2 n_halo. */
+void euler1d_gpu_upload(euler1d_gpu_t* solver, const double* h_data);
+/* euler1d_solver.hpp:49. */
+void euler1d_gpu_download(euler1d_gpu_t* solver, double* h_data);
+/* euler1d_solver.hpp:58: cfl * dx / max(|u| + c) over the interior. */
+double euler1d_gpu_compute_dt(euler1d_gpu_t* solver, double cfl);
+/* euler1d_solver.hpp:66: one Heun step with the given dt. */
+void euler1d_gpu_rk2_step(euler1d_gpu_t* solver, double dt);
+/* euler1d_solver.hpp:76: run from time 0 until t_final; returns the step count (-1 on error). */
+int euler1d_gpu_run(euler1d_gpu_t* solver, double t_final, double cfl);
+/* euler1d_solver.hpp:87: as run, returns wall-clock milliseconds. */
+double euler1d_gpu_run_timed(euler1d_gpu_t* solver, double t_final, double cfl, int* steps);
+
+/* Extensions on the same handle (no counterpart in nest's ABI). */
+nest_status euler1d_gpu_set_bc(euler1d_gpu_t* solver, int bc);
+/* Status of the last call made on this handle. */
+nest_status euler1d_gpu_status(euler1d_gpu_t* solver);
+
+/* ------------------------------------------------------------------------ */
+/* Solver API: 1D / 2D, FP64 plain or FP32 form, one domain per handle.     */
+/* Replaces the time loops of examples/benchmark/benchmark_euler1d.cpp:     */
+/* 185-209 and examples/sod2d/sod2d.cpp:318-366 on the device.  A step is   */
+/* dt (CFL max-reduction on the device) -> ghost fill -> stage 1 -> ghost   */
+/* fill -> stage 2 + Heun average, with no host synchronisation.            */
+/* ------------------------------------------------------------------------ */
+
+typedef struct nest_solver nest_solver;
+
+typedef struct nest_solver_desc {
+    int dim;          /* 1 or 2 */
+    int nx, ny;       /* interior cells (ny unused for dim 1) */
+    int halo;         /* ghost width: 2 (dim 1 accepts >= 2) */
+    double dx, dy;    /* cell sizes (dy unused for dim 1) */
+    double gamma;
+    int bc_x, bc_y;   /* NEST_BC_* */
+    int precision;    /* NEST_F64 or NEST_F32 (dim 2 only) */
+    int flags;        /* NEST_FLAG_* */
+    void* stream;     /* cudaStream_t to run on, or NULL for a private stream */
+} nest_solver_desc;
+
+nest_status nest_solver_create(const nest_solver_desc* desc, nest_solver** out);
+nest_status nest_solver_destroy(nest_solver* s);
+/* Host arrays are in the solver precision (double for F64, float for F32). */
+nest_status nest_solver_upload(nest_solver* s, const void* host, int layout);
+nest_status nest_solver_download(nest_solver* s, void* host, int layout);
+/* Same with a device pointer (e.g. a torch tensor); no host staging. */
+nest_status nest_solver_upload_device(nest_solver* s, const void* dev, int layout);
+nest_status nest_solver_download_device(nest_solver* s, void* dev, int layout);
+/* Enqueue nsteps steps with CFL dt; returns without waiting. */
+nest_status nest_solver_step(nest_solver* s, int nsteps, double cfl);
+/* nsteps CFL steps launched one kernel at a time with a CUDA event between
+ * kernels on the solver stream (no graph); waits.  stage_ms (2*nsteps, may be
+ * NULL) receives each kernel's duration in launch order, total_ms the span. */
+nest_status nest_solver_step_profiled(nest_solver* s, int nsteps, double cfl, float* stage_ms, float* total_ms);
+/* Enqueue nsteps steps with a fixed dt (nest's rk2_step(dt)). */
+nest_status nest_solver_step_dt(nest_solver* s, int nsteps, double dt);
+/* Advance until time >= t_final (dt clamped to hit it) or max_steps (> 0)
+ * more steps; waits.  *steps_out = steps taken by this call. */
+nest_status nest_solver_run_to(nest_solver* s, double t_final, double cfl, int max_steps, int* steps_out);
+/* dt = CFL rule on the current state (waits). */
+nest_status nest_solver_compute_dt(nest_solver* s, double cfl, double* dt_out);
+/* Simulated time and completed steps since creation / last reset (waits). */
+nest_status nest_solver_time(nest_solver* s, double* time, int* steps);
+nest_status nest_solver_reset_time(nest_solver* s);
+/* FP64 conserved totals of the state after the last step (2D, needs
+ * NEST_FLAG_TOTALS): sum of rho, rho u, rho v, E over the interior times dx dy. */
+nest_status nest_solver_totals(nest_solver* s, double out[4]);
+/* Number of cells repaired by the FP32 form so far. */
+nest_status nest_solver_repairs(nest_solver* s, unsigned* count);
+nest_status nest_solver_sync(nest_solver* s);
+/* 2D launch shape: rows per tile and warps per block (autotuner hook). */
+nest_status nest_solver_set_tiling(nest_solver* s, int rows_per_tile, int warps_per_block);
+/* dt sequence: mode 0 freezes the given n values (copied), mode 1 records the
+ * next n dts (read back with nest_solver_get_dts), mode 2 clears. */
+nest_status nest_solver_set_dt_sequence(nest_solver* s, const double* dts, int n, int mode);
+nest_status nest_solver_get_dts(nest_solver* s, double* dts, int n);
+/* Device state: base pointer, row pitch (elements) and plane stride (elements). */
+nest_status nest_solver_state_ptr(nest_solver* s, void** dev, long long* pitch, long long* vstride);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEST_B200_H */

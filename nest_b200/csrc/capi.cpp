@@ -1,0 +1,679 @@
+// Host runtime and C ABI of the nest B200 hot path (C++20).
+//
+// One nest_solver owns its device state (U, the stage buffer U1, a StepCtrl
+// control block and optional per-warp totals) and a stream.  Steps are
+// enqueued without host synchronisation: dt is derived on the device from
+// the wave-speed maximum that the previous stage 2 reduced, and runs of steps
+// are captured once into CUDA graphs and replayed.
+//
+// The euler1d_gpu_* functions keep the names, signatures and semantics of
+// nest's C ABI (src/backend_cuda/euler1d_solver.hpp:16-87,
+// src/backend_cuda/euler1d_solver.cu:159-235) on top of a 1D FP64 solver.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <tuple>
+
+#include "../../include/nest_b200.h"
+#include "common.cuh"
+#include "euler2d_kernels.cuh"
+#include "kernels.h"
+
+using namespace nestb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+nest_status fail(nest_status st, const std::string& msg) {
+    g_last_error = msg;
+    return st;
+}
+
+nest_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? NEST_ERR_OOM : NEST_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t e__ = (call);                             \
+        if (e__ != cudaSuccess) return cuda_fail(e__, #call); \
+    } while (0)
+
+double bits_to_double(unsigned long long b) {
+    double d;
+    std::memcpy(&d, &b, sizeof d);
+    return d;
+}
+
+constexpr int GRAPH_STEPS = 16;  // steps per captured graph (even: parity-neutral)
+
+struct GraphKey {
+    int nsteps, parity;
+    double cfl, t_final, fixed_dt;
+    int max_steps;
+    const double* dts_in;
+    double* dts_out;
+    int dts_cap, tx, warps;
+    bool operator<(const GraphKey& o) const {
+        return std::tie(nsteps, parity, cfl, t_final, fixed_dt, max_steps, dts_in, dts_out, dts_cap, tx, warps) <
+               std::tie(o.nsteps, o.parity, o.cfl, o.t_final, o.fixed_dt, o.max_steps, o.dts_in, o.dts_out,
+                        o.dts_cap, o.tx, o.warps);
+    }
+};
+
+}  // namespace
+
+struct nest_solver {
+    nest_solver_desc d{};
+    int h = 2;
+    int n_total = 0;           // 1D: n + 2h
+    int pitch = 0;             // 2D: elements per row
+    long long vstride = 0;     // elements per variable plane
+    int nvars = 3;
+    size_t esize = 8;
+    void* U = nullptr;
+    void* U1 = nullptr;
+    StepCtrl* ctrl = nullptr;
+    StepCtrl* host_ctrl = nullptr;   // pinned mirror
+    double* partials = nullptr;
+    long long nrec = 0;
+    double* totals_dev = nullptr;
+    double* dts_in = nullptr;
+    double* dts_out = nullptr;
+    int dts_cap = 0;
+    int dts_mode = 2;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    int parity = 0;
+    bool prepared = false;
+    int tx = 64, warps = 4;
+    std::map<GraphKey, cudaGraphExec_t> graphs;
+
+    bool resident() const {
+        return d.dim == 1 && !(d.flags & NEST_FLAG_NO_RESIDENT) &&
+               resident_smem_bytes(d.nx, h) <= 220 * 1024;
+    }
+    Geo2D geo() const {
+        Geo2D g;
+        g.nx = d.nx; g.ny = d.ny; g.pitch = pitch; g.vstride = vstride;
+        g.bcx = d.bc_x; g.bcy = d.bc_y; g.dx = d.dx; g.dy = d.dy; g.gamma = d.gamma;
+        return g;
+    }
+    size_t state_bytes() const { return esize * (size_t)nvars * (size_t)vstride; }
+};
+
+namespace {
+
+nest_status drop_graphs(nest_solver* s) {
+    for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    return NEST_OK;
+}
+
+LoopParams base_params(const nest_solver* s) {
+    LoopParams lp{};
+    lp.dts_in = (s->dts_mode == 0) ? s->dts_in : nullptr;
+    lp.dts_out = (s->dts_mode == 1) ? s->dts_out : nullptr;
+    lp.dts_cap = s->dts_cap;
+    return lp;
+}
+
+// Ghost fill + wave-speed maxima of the current state into slot `parity`.
+nest_status prepare(nest_solver* s) {
+    CK(cudaMemsetAsync(&s->ctrl->maxs[s->parity][0], 0, 2 * sizeof(unsigned long long), s->st));
+    cudaError_t e;
+    if (s->d.dim == 1) {
+        e = launch_1d_prepare((double*)s->U, s->d.nx, s->h, s->d.gamma, s->d.bc_x, s->ctrl, s->parity, s->st);
+    } else if (s->d.precision == NEST_F64) {
+        e = launch_2d_prepare_f64((double*)s->U, s->geo(), s->ctrl, s->parity, s->st);
+    } else {
+        e = launch_2d_prepare_f32((float*)s->U, s->geo(), s->ctrl, s->parity, s->st);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "prepare kernel");
+    s->prepared = true;
+    return NEST_OK;
+}
+
+// Enqueue one step (two kernels) with parity p; `which` selects the stages.
+cudaError_t enqueue_step(nest_solver* s, const LoopParams& lp, int p, int which = 3) {
+    if (s->d.dim == 1)
+        return launch_1d_step((double*)s->U, (double*)s->U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp,
+                              s->ctrl, p, which, s->st);
+    if (s->d.precision == NEST_F64)
+        return launch_2d_step_f64((double*)s->U, (double*)s->U1, s->geo(), lp, s->ctrl, s->partials, p, s->tx,
+                                  s->warps, which, s->st);
+    return launch_2d_step_f32((float*)s->U, (float*)s->U1, s->geo(), lp, s->ctrl, s->partials, p, s->tx, s->warps,
+                              (s->d.flags & NEST_FLAG_REPAIR) != 0, which, s->st);
+}
+
+// Enqueue nsteps steps of the tiled path; whole chunks go through cached graphs.
+nest_status enqueue_steps(nest_solver* s, int nsteps, const LoopParams& lp) {
+    if (!s->prepared) {
+        nest_status r = prepare(s);
+        if (r != NEST_OK) return r;
+    }
+    bool use_graphs = s->st != nullptr;
+    while (nsteps > 0) {
+        if (use_graphs && nsteps >= GRAPH_STEPS) {
+            GraphKey k{GRAPH_STEPS, s->parity, lp.cfl, lp.t_final, lp.fixed_dt, lp.max_steps, lp.dts_in,
+                       lp.dts_out, lp.dts_cap, s->tx, s->warps};
+            auto it = s->graphs.find(k);
+            if (it == s->graphs.end()) {
+                cudaGraph_t g;
+                CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+                int p = s->parity;
+                cudaError_t e = cudaSuccess;
+                for (int i = 0; i < GRAPH_STEPS && e == cudaSuccess; ++i, p ^= 1) e = enqueue_step(s, lp, p);
+                cudaError_t e2 = cudaStreamEndCapture(s->st, &g);
+                if (e != cudaSuccess) return cuda_fail(e, "step capture");
+                if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+                cudaGraphExec_t ge;
+                cudaError_t e3 = cudaGraphInstantiate(&ge, g, 0);
+                cudaGraphDestroy(g);
+                if (e3 != cudaSuccess) return cuda_fail(e3, "cudaGraphInstantiate");
+                it = s->graphs.emplace(k, ge).first;
+            }
+            CK(cudaGraphLaunch(it->second, s->st));
+            nsteps -= GRAPH_STEPS;  // parity unchanged (even chunk)
+        } else {
+            cudaError_t e = enqueue_step(s, lp, s->parity);
+            if (e != cudaSuccess) return cuda_fail(e, "step launch");
+            s->parity ^= 1;
+            --nsteps;
+        }
+    }
+    return NEST_OK;
+}
+
+nest_status read_ctrl(nest_solver* s) {
+    CK(cudaMemcpyAsync(s->host_ctrl, s->ctrl, sizeof(StepCtrl), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (s->host_ctrl->err & ERRW_NONFINITE) return fail(NEST_ERR_NUMERIC, "non-finite wave speed: the state blew up");
+    return NEST_OK;
+}
+
+// Advance by at most `budget` steps (<= 0: unbounded) with the given loop
+// parameters; on the resident 1D path this is a single launch.
+nest_status advance(nest_solver* s, LoopParams lp, int budget) {
+    if (s->resident()) {
+        lp.step_budget = budget;
+        cudaError_t e = launch_1d_resident((double*)s->U, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp,
+                                           s->ctrl, s->parity, s->st);
+        if (e != cudaSuccess) return cuda_fail(e, "resident solver launch");
+        s->prepared = false;  // the resident kernel does not leave maxs behind
+        return NEST_OK;
+    }
+    return enqueue_steps(s, budget, lp);
+}
+
+nest_status check(const nest_solver* s) {
+    if (!s) return fail(NEST_ERR_INVALID, "null solver handle");
+    return NEST_OK;
+}
+
+nest_status copy_state(nest_solver* s, void* dst, const void* src, int layout, bool upload, cudaMemcpyKind kind) {
+    if (layout != NEST_LAYOUT_EXTENDED && layout != NEST_LAYOUT_INTERIOR)
+        return fail(NEST_ERR_INVALID, "unknown layout");
+    size_t es = s->esize;
+    if (s->d.dim == 1) {
+        int n = s->d.nx, nt = s->n_total;
+        if (layout == NEST_LAYOUT_EXTENDED) {
+            if (upload) CK(cudaMemcpyAsync(s->U, src, es * 3 * nt, kind, s->st));
+            else CK(cudaMemcpyAsync(dst, s->U, es * 3 * nt, kind, s->st));
+        } else {
+            // interior rows: 3 planes of n with the device plane stride nt
+            if (upload)
+                CK(cudaMemcpy2DAsync((char*)s->U + es * s->h, es * nt, src, es * n, es * n, 3, kind, s->st));
+            else
+                CK(cudaMemcpy2DAsync(dst, es * n, (char*)s->U + es * s->h, es * nt, es * n, 3, kind, s->st));
+        }
+        return NEST_OK;
+    }
+    int nx = s->d.nx, ny = s->d.ny;
+    int rows = (layout == NEST_LAYOUT_EXTENDED) ? nx + 4 : nx;
+    int cols = (layout == NEST_LAYOUT_EXTENDED) ? ny + 4 : ny;
+    size_t off = (layout == NEST_LAYOUT_EXTENDED) ? 0 : (size_t)(2 * s->pitch + 2);
+    for (int k = 0; k < 4; ++k) {
+        char* dev = (char*)s->U + es * ((size_t)k * s->vstride + off);
+        size_t hoff = es * (size_t)k * rows * cols;
+        if (upload)
+            CK(cudaMemcpy2DAsync(dev, es * s->pitch, (const char*)src + hoff, es * cols, es * cols, rows, kind, s->st));
+        else
+            CK(cudaMemcpy2DAsync((char*)dst + hoff, es * cols, dev, es * s->pitch, es * cols, rows, kind, s->st));
+    }
+    return NEST_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Solver API
+// ===========================================================================
+
+extern "C" {
+
+const char* nest_last_error(void) { return g_last_error.c_str(); }
+
+int nest_version(void) { return 10000; }
+
+nest_status nest_solver_create(const nest_solver_desc* d, nest_solver** out) {
+    if (!d || !out) return fail(NEST_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (d->dim != 1 && d->dim != 2) return fail(NEST_ERR_INVALID, "dim must be 1 or 2");
+    if (d->nx < 4 || (d->dim == 2 && d->ny < 4)) return fail(NEST_ERR_INVALID, "need at least 4 interior cells per axis");
+    if (!(d->dx > 0.0) || (d->dim == 2 && !(d->dy > 0.0))) return fail(NEST_ERR_INVALID, "cell sizes must be positive");
+    if (!(d->gamma > 1.0)) return fail(NEST_ERR_INVALID, "gamma must exceed 1");
+    if (d->bc_x != NEST_BC_PERIODIC && d->bc_x != NEST_BC_OUTFLOW) return fail(NEST_ERR_INVALID, "bad bc_x");
+    if (d->dim == 2 && d->bc_y != NEST_BC_PERIODIC && d->bc_y != NEST_BC_OUTFLOW) return fail(NEST_ERR_INVALID, "bad bc_y");
+    if (d->dim == 1 && d->halo < 2) return fail(NEST_ERR_INVALID, "PLM needs a halo of at least 2");
+    if (d->dim == 2 && d->halo != 2) return fail(NEST_ERR_UNSUPPORTED, "2D solver uses a halo of exactly 2");
+    if (d->dim == 1 && d->precision != NEST_F64) return fail(NEST_ERR_UNSUPPORTED, "1D solver is FP64");
+    if (d->precision != NEST_F64 && d->precision != NEST_F32) return fail(NEST_ERR_INVALID, "bad precision");
+    if (d->dim == 2 && (long long)d->nx * d->ny > (1ll << 31)) return fail(NEST_ERR_INVALID, "domain too large");
+
+    nest_solver* s = new (std::nothrow) nest_solver;
+    if (!s) return fail(NEST_ERR_OOM, "host allocation failed");
+    s->d = *d;
+    s->h = d->halo;
+    s->esize = d->precision == NEST_F64 ? 8 : 4;
+    if (d->dim == 1) {
+        s->nvars = 3;
+        s->n_total = d->nx + 2 * d->halo;
+        s->vstride = s->n_total;
+        s->pitch = s->n_total;
+    } else {
+        s->nvars = 4;
+        int align = (int)(128 / s->esize);  // rows start on 128-byte boundaries
+        s->pitch = ((d->ny + 4 + align - 1) / align) * align;
+        s->vstride = (long long)s->pitch * (d->nx + 4);
+        long long pad = 256 / (long long)s->esize;
+        s->vstride = ((s->vstride + pad - 1) / pad) * pad;
+    }
+    auto cleanup = [&](nest_status st) { nest_solver_destroy(s); return st; };
+    cudaError_t e;
+    if (d->stream) {
+        s->st = (cudaStream_t)d->stream;
+    } else {
+        e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaStreamCreate"));
+        s->own_stream = true;
+    }
+    size_t bytes = s->state_bytes();
+    if ((e = cudaMalloc(&s->U, bytes)) != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(U)"));
+    if ((e = cudaMalloc(&s->U1, bytes)) != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(U1)"));
+    if ((e = cudaMalloc(&s->ctrl, sizeof(StepCtrl))) != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(ctrl)"));
+    if ((e = cudaMallocHost(&s->host_ctrl, sizeof(StepCtrl))) != cudaSuccess) return cleanup(cuda_fail(e, "cudaMallocHost"));
+    if ((e = cudaMemsetAsync(s->U, 0, bytes, s->st)) != cudaSuccess) return cleanup(cuda_fail(e, "memset"));
+    if ((e = cudaMemsetAsync(s->U1, 0, bytes, s->st)) != cudaSuccess) return cleanup(cuda_fail(e, "memset"));
+    if ((e = cudaMemsetAsync(s->ctrl, 0, sizeof(StepCtrl), s->st)) != cudaSuccess) return cleanup(cuda_fail(e, "memset"));
+    if (d->dim == 2 && (d->flags & NEST_FLAG_TOTALS)) {
+        long long nstrips = (d->ny + STRIP - 1) / STRIP;
+        // sized for the smallest tile height the tiling hook accepts (8 rows)
+        s->nrec = nstrips * ((d->nx + 7) / 8);
+        if ((e = cudaMalloc(&s->partials, sizeof(double) * 4 * s->nrec)) != cudaSuccess)
+            return cleanup(cuda_fail(e, "cudaMalloc(partials)"));
+        if ((e = cudaMemsetAsync(s->partials, 0, sizeof(double) * 4 * s->nrec, s->st)) != cudaSuccess)
+            return cleanup(cuda_fail(e, "memset"));
+        if ((e = cudaMalloc(&s->totals_dev, sizeof(double) * 4)) != cudaSuccess)
+            return cleanup(cuda_fail(e, "cudaMalloc(totals)"));
+    }
+    if ((e = cudaStreamSynchronize(s->st)) != cudaSuccess) return cleanup(cuda_fail(e, "sync"));
+    *out = s;
+    return NEST_OK;
+}
+
+nest_status nest_solver_destroy(nest_solver* s) {
+    if (!s) return NEST_OK;
+    if (s->st) cudaStreamSynchronize(s->st);
+    drop_graphs(s);
+    cudaFree(s->U); cudaFree(s->U1); cudaFree(s->ctrl); cudaFree(s->partials); cudaFree(s->totals_dev);
+    cudaFree(s->dts_in); cudaFree(s->dts_out);
+    if (s->host_ctrl) cudaFreeHost(s->host_ctrl);
+    if (s->own_stream && s->st) cudaStreamDestroy(s->st);
+    delete s;
+    return NEST_OK;
+}
+
+static nest_status upload_impl(nest_solver* s, const void* src, int layout, cudaMemcpyKind kind) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (!src) return fail(NEST_ERR_INVALID, "null source");
+    r = copy_state(s, nullptr, src, layout, true, kind);
+    if (r != NEST_OK) return r;
+    r = prepare(s);
+    if (r != NEST_OK) return r;
+    CK(cudaStreamSynchronize(s->st));
+    return NEST_OK;
+}
+
+static nest_status download_impl(nest_solver* s, void* dst, int layout, cudaMemcpyKind kind) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (!dst) return fail(NEST_ERR_INVALID, "null destination");
+    r = copy_state(s, dst, nullptr, layout, false, kind);
+    if (r != NEST_OK) return r;
+    CK(cudaStreamSynchronize(s->st));
+    return NEST_OK;
+}
+
+nest_status nest_solver_upload(nest_solver* s, const void* host, int layout) {
+    return upload_impl(s, host, layout, cudaMemcpyHostToDevice);
+}
+nest_status nest_solver_download(nest_solver* s, void* host, int layout) {
+    return download_impl(s, host, layout, cudaMemcpyDeviceToHost);
+}
+nest_status nest_solver_upload_device(nest_solver* s, const void* dev, int layout) {
+    return upload_impl(s, dev, layout, cudaMemcpyDeviceToDevice);
+}
+nest_status nest_solver_download_device(nest_solver* s, void* dev, int layout) {
+    return download_impl(s, dev, layout, cudaMemcpyDeviceToDevice);
+}
+
+nest_status nest_solver_step(nest_solver* s, int nsteps, double cfl) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (nsteps < 0) return fail(NEST_ERR_INVALID, "negative step count");
+    if (!(cfl > 0.0)) return fail(NEST_ERR_INVALID, "cfl must be positive");
+    if (nsteps == 0) return NEST_OK;
+    LoopParams lp = base_params(s);
+    lp.cfl = cfl;
+    return advance(s, lp, nsteps);
+}
+
+nest_status nest_solver_step_profiled(nest_solver* s, int nsteps, double cfl, float* stage_ms, float* total_ms) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (nsteps <= 0 || !(cfl > 0.0)) return fail(NEST_ERR_INVALID, "need nsteps > 0 and cfl > 0");
+    if (s->resident()) return fail(NEST_ERR_UNSUPPORTED, "profiled steps use the tiled path (NEST_FLAG_NO_RESIDENT)");
+    if (!s->prepared && (r = prepare(s)) != NEST_OK) return r;
+    LoopParams lp = base_params(s);
+    lp.cfl = cfl;
+    int nev = 2 * nsteps + 1;
+    cudaEvent_t* ev = new (std::nothrow) cudaEvent_t[nev];
+    if (!ev) return fail(NEST_ERR_OOM, "host allocation failed");
+    int made = 0;
+    cudaError_t e = cudaSuccess;
+    for (; made < nev && e == cudaSuccess; ++made) e = cudaEventCreate(&ev[made]);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[0], s->st);
+    for (int i = 0; i < nsteps && e == cudaSuccess; ++i) {
+        e = enqueue_step(s, lp, s->parity, 1);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[2 * i + 1], s->st);
+        if (e == cudaSuccess) e = enqueue_step(s, lp, s->parity, 2);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[2 * i + 2], s->st);
+        s->parity ^= 1;
+    }
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev[nev - 1]);
+    for (int i = 0; i < 2 * nsteps && e == cudaSuccess; ++i) {
+        float ms = 0.f;
+        e = cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+        if (stage_ms) stage_ms[i] = ms;
+    }
+    if (e == cudaSuccess && total_ms) e = cudaEventElapsedTime(total_ms, ev[0], ev[nev - 1]);
+    for (int i = 0; i < made; ++i) cudaEventDestroy(ev[i]);
+    delete[] ev;
+    if (e != cudaSuccess) return cuda_fail(e, "profiled steps");
+    return read_ctrl(s);
+}
+
+nest_status nest_solver_step_dt(nest_solver* s, int nsteps, double dt) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (nsteps < 0) return fail(NEST_ERR_INVALID, "negative step count");
+    if (!(dt > 0.0)) return fail(NEST_ERR_INVALID, "dt must be positive");
+    if (nsteps == 0) return NEST_OK;
+    LoopParams lp = base_params(s);
+    lp.cfl = 1.0;
+    lp.fixed_dt = dt;
+    lp.dts_in = nullptr;
+    return advance(s, lp, nsteps);
+}
+
+nest_status nest_solver_run_to(nest_solver* s, double t_final, double cfl, int max_steps, int* steps_out) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (!(cfl > 0.0) || !(t_final > 0.0)) return fail(NEST_ERR_INVALID, "cfl and t_final must be positive");
+    if ((r = read_ctrl(s)) != NEST_OK) return r;
+    int start = s->host_ctrl->step[s->parity];
+    LoopParams lp = base_params(s);
+    lp.cfl = cfl;
+    lp.t_final = t_final;
+    lp.max_steps = max_steps > 0 ? start + max_steps : 0;
+    if (s->resident()) {
+        if ((r = advance(s, lp, 0)) != NEST_OK) return r;
+        if ((r = read_ctrl(s)) != NEST_OK) return r;
+    } else {
+        const int chunk = 4 * GRAPH_STEPS;
+        for (;;) {
+            if ((r = enqueue_steps(s, chunk, lp)) != NEST_OK) return r;
+            if ((r = read_ctrl(s)) != NEST_OK) return r;
+            const StepCtrl* c = s->host_ctrl;
+            int p = s->parity;
+            if (!(c->time[p] < t_final)) break;
+            if (lp.max_steps > 0 && c->step[p] >= lp.max_steps) break;
+            if (s->dts_mode == 0 && c->step[p] >= s->dts_cap) break;
+        }
+    }
+    if (steps_out) *steps_out = s->host_ctrl->step[s->parity] - start;
+    return NEST_OK;
+}
+
+nest_status nest_solver_compute_dt(nest_solver* s, double cfl, double* dt_out) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (!dt_out) return fail(NEST_ERR_INVALID, "null output");
+    if ((r = prepare(s)) != NEST_OK) return r;
+    if ((r = read_ctrl(s)) != NEST_OK) return r;
+    double sx = bits_to_double(s->host_ctrl->maxs[s->parity][0]);
+    if (s->d.dim == 1) {
+        *dt_out = cfl * s->d.dx / sx;  // benchmark_euler1d.cpp:179
+    } else {
+        double sy = bits_to_double(s->host_ctrl->maxs[s->parity][1]);
+        double dtx = 1e10, dty = 1e10;  // euler2d.hpp:249-270
+        if (sx > 0.0 && s->d.dx / sx < dtx) dtx = s->d.dx / sx;
+        if (sy > 0.0 && s->d.dy / sy < dty) dty = s->d.dy / sy;
+        *dt_out = cfl * (dty < dtx ? dty : dtx);
+    }
+    return NEST_OK;
+}
+
+nest_status nest_solver_time(nest_solver* s, double* time, int* steps) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if ((r = read_ctrl(s)) != NEST_OK) return r;
+    if (time) *time = s->host_ctrl->time[s->parity];
+    if (steps) *steps = s->host_ctrl->step[s->parity];
+    return NEST_OK;
+}
+
+nest_status nest_solver_reset_time(nest_solver* s) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    CK(cudaStreamSynchronize(s->st));
+    CK(cudaMemcpyAsync(s->host_ctrl, s->ctrl, sizeof(StepCtrl), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    for (int p = 0; p < 2; ++p) { s->host_ctrl->time[p] = 0.0; s->host_ctrl->step[p] = 0; }
+    CK(cudaMemcpyAsync(s->ctrl, s->host_ctrl, sizeof(StepCtrl), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return NEST_OK;
+}
+
+nest_status nest_solver_totals(nest_solver* s, double out[4]) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (!s->partials) return fail(NEST_ERR_UNSUPPORTED, "totals need a 2D solver created with NEST_FLAG_TOTALS");
+    cudaError_t e = launch_sum_partials(s->partials, s->nrec, s->totals_dev, s->st);
+    if (e != cudaSuccess) return cuda_fail(e, "totals kernel");
+    CK(cudaMemcpyAsync(out, s->totals_dev, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    for (int k = 0; k < 4; ++k) out[k] *= s->d.dx * s->d.dy;
+    return NEST_OK;
+}
+
+nest_status nest_solver_repairs(nest_solver* s, unsigned* count) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if ((r = read_ctrl(s)) != NEST_OK) return r;
+    if (count) *count = s->host_ctrl->repairs;
+    return NEST_OK;
+}
+
+nest_status nest_solver_sync(nest_solver* s) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    return read_ctrl(s);
+}
+
+nest_status nest_solver_set_tiling(nest_solver* s, int rows_per_tile, int warps_per_block) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (rows_per_tile < 8 || rows_per_tile > 4096) return fail(NEST_ERR_INVALID, "rows per tile must be in [8, 4096]");
+    if (warps_per_block < 1 || warps_per_block > 8) return fail(NEST_ERR_INVALID, "warps per block must be in [1, 8]");
+    s->tx = rows_per_tile;
+    s->warps = warps_per_block;
+    if (s->partials) cudaMemsetAsync(s->partials, 0, sizeof(double) * 4 * s->nrec, s->st);
+    return NEST_OK;
+}
+
+nest_status nest_solver_set_dt_sequence(nest_solver* s, const double* dts, int n, int mode) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    CK(cudaStreamSynchronize(s->st));
+    drop_graphs(s);
+    cudaFree(s->dts_in); s->dts_in = nullptr;
+    cudaFree(s->dts_out); s->dts_out = nullptr;
+    s->dts_cap = 0;
+    s->dts_mode = 2;
+    if (mode == 2) return NEST_OK;
+    if (n <= 0) return fail(NEST_ERR_INVALID, "sequence length must be positive");
+    if (mode == 0) {
+        if (!dts) return fail(NEST_ERR_INVALID, "null dt sequence");
+        CK(cudaMalloc(&s->dts_in, sizeof(double) * n));
+        CK(cudaMemcpy(s->dts_in, dts, sizeof(double) * n, cudaMemcpyHostToDevice));
+    } else if (mode == 1) {
+        CK(cudaMalloc(&s->dts_out, sizeof(double) * n));
+        CK(cudaMemset(s->dts_out, 0, sizeof(double) * n));
+    } else {
+        return fail(NEST_ERR_INVALID, "mode must be 0, 1 or 2");
+    }
+    s->dts_cap = n;
+    s->dts_mode = mode;
+    return NEST_OK;
+}
+
+nest_status nest_solver_get_dts(nest_solver* s, double* dts, int n) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (s->dts_mode != 1) return fail(NEST_ERR_INVALID, "no dt recording active");
+    if (n > s->dts_cap) n = s->dts_cap;
+    CK(cudaMemcpyAsync(dts, s->dts_out, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return NEST_OK;
+}
+
+nest_status nest_solver_state_ptr(nest_solver* s, void** dev, long long* pitch, long long* vstride) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (dev) *dev = s->U;
+    if (pitch) *pitch = s->pitch;
+    if (vstride) *vstride = s->vstride;
+    return NEST_OK;
+}
+
+// ===========================================================================
+// nest-compatible 1D ABI
+// ===========================================================================
+
+struct euler1d_gpu_t {
+    nest_solver* s = nullptr;
+    nest_status last = NEST_OK;
+};
+
+static nest_status note(euler1d_gpu_t* h, nest_status st) {
+    if (h) h->last = st;
+    return st;
+}
+
+euler1d_gpu_t* euler1d_gpu_create(int n_interior, int n_halo, double dx, double gamma) {
+    nest_solver_desc d{};
+    d.dim = 1; d.nx = n_interior; d.ny = 1; d.halo = n_halo;
+    d.dx = dx; d.dy = dx; d.gamma = gamma;
+    d.bc_x = NEST_BC_PERIODIC; d.bc_y = NEST_BC_PERIODIC;  // nest's solver is periodic (euler1d_cuda.cuh:337-360)
+    d.precision = NEST_F64;
+    auto* h = new (std::nothrow) euler1d_gpu_t;
+    if (!h) { fail(NEST_ERR_OOM, "host allocation failed"); return nullptr; }
+    if (nest_solver_create(&d, &h->s) != NEST_OK) { delete h; return nullptr; }
+    return h;
+}
+
+void euler1d_gpu_destroy(euler1d_gpu_t* h) {
+    if (!h) return;
+    nest_solver_destroy(h->s);
+    delete h;
+}
+
+void euler1d_gpu_upload(euler1d_gpu_t* h, const double* h_data) {
+    if (!h) { fail(NEST_ERR_INVALID, "null solver handle"); return; }
+    note(h, nest_solver_upload(h->s, h_data, NEST_LAYOUT_EXTENDED));
+}
+
+void euler1d_gpu_download(euler1d_gpu_t* h, double* h_data) {
+    if (!h) { fail(NEST_ERR_INVALID, "null solver handle"); return; }
+    note(h, nest_solver_download(h->s, h_data, NEST_LAYOUT_EXTENDED));
+}
+
+double euler1d_gpu_compute_dt(euler1d_gpu_t* h, double cfl) {
+    if (!h) { fail(NEST_ERR_INVALID, "null solver handle"); return 0.0; }
+    double dt = 0.0;
+    note(h, nest_solver_compute_dt(h->s, cfl, &dt));
+    return dt;
+}
+
+void euler1d_gpu_rk2_step(euler1d_gpu_t* h, double dt) {
+    if (!h) { fail(NEST_ERR_INVALID, "null solver handle"); return; }
+    nest_status r = nest_solver_step_dt(h->s, 1, dt);
+    if (r == NEST_OK) r = nest_solver_sync(h->s);
+    note(h, r);
+}
+
+int euler1d_gpu_run(euler1d_gpu_t* h, double t_final, double cfl) {
+    if (!h) { fail(NEST_ERR_INVALID, "null solver handle"); return -1; }
+    // nest's run() starts its own clock at 0 on every call (euler1d_solver.cu:159-174).
+    nest_status r = nest_solver_reset_time(h->s);
+    int steps = 0;
+    if (r == NEST_OK) r = nest_solver_run_to(h->s, t_final, cfl, 0, &steps);
+    note(h, r);
+    return r == NEST_OK ? steps : -1;
+}
+
+double euler1d_gpu_run_timed(euler1d_gpu_t* h, double t_final, double cfl, int* steps) {
+    if (!h) { fail(NEST_ERR_INVALID, "null solver handle"); return -1.0; }
+    nest_solver_sync(h->s);
+    auto t0 = std::chrono::high_resolution_clock::now();
+    int n = euler1d_gpu_run(h, t_final, cfl);
+    auto t1 = std::chrono::high_resolution_clock::now();
+    if (steps) *steps = n;
+    return std::chrono::duration<double, std::milli>(t1 - t0).count();
+}
+
+nest_status euler1d_gpu_set_bc(euler1d_gpu_t* h, int bc) {
+    if (!h) return fail(NEST_ERR_INVALID, "null solver handle");
+    if (bc != NEST_BC_PERIODIC && bc != NEST_BC_OUTFLOW) return note(h, fail(NEST_ERR_INVALID, "bad bc"));
+    h->s->d.bc_x = bc;
+    h->s->prepared = false;
+    drop_graphs(h->s);
+    return note(h, NEST_OK);
+}
+
+nest_status euler1d_gpu_status(euler1d_gpu_t* h) {
+    if (!h) return NEST_ERR_INVALID;
+    return h->last;
+}
+
+}  // extern "C"

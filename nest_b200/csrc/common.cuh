@@ -1,0 +1,172 @@
+// Shared device definitions for the nest B200 kernels.
+//
+// Precision policy
+//   double : the plain form.  Every translation unit that instantiates it is
+//            compiled with -fmad=false and IEEE division / square root, and
+//            the formulas below keep the operation order of nest's CPU code
+//            (examples/sod1d/euler1d.hpp), so results match the CPU path bit
+//            for bit.
+//   float  : the FP32 form (reconstruction, Riemann solve and update in
+//            FP32; totals, time and positivity repair in FP64).  Its
+//            translation unit is compiled with FMA contraction and fast
+//            reciprocal / square-root approximations.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nestb {
+
+// Boundary conditions on the domain edges.
+enum { BC_PERIODIC = 0, BC_OUTFLOW = 1 };
+
+// Device error word bits (read back by the host after a run).
+enum : unsigned {
+    ERRW_NONFINITE = 1u,   // a wave speed was NaN/Inf
+    ERRW_NONPOSITIVE = 2u, // rho or p below zero after the update (FP64 form)
+    ERRW_TIMEOUT = 4u,     // a bounded spin gave up
+    ERRW_REPAIRED = 8u,    // FP32 form: positivity repair was applied
+};
+
+// Per-solver control block in device memory.  Fields indexed [p] belong to
+// the step launched with parity p; a step with parity p reads slot p and
+// prepares slot 1-p, so the two kernels of a step never race on a field.
+struct StepCtrl {
+    double time[2];                 // simulated time at the start of the step
+    double dt[2];                   // dt chosen by stage 1 of the step
+    unsigned long long maxs[2][2];  // [p][axis] max wave speed of U at the start of step p (bits of a non-negative double)
+    int step[2];                    // completed steps at the start of the step
+    int active[2];                  // stage 1 sets it: 1 = the step runs, 0 = finished
+    unsigned err;                   // ERRW_* bits
+    unsigned repairs;               // FP32 form: number of repaired cells
+};
+
+// Time-loop parameters shared by all launches of a solver.
+struct LoopParams {
+    double cfl;
+    double t_final;        // > 0: stop when time >= t_final and clamp dt
+    int max_steps;         // > 0: stop after this many steps
+    const double* dts_in;  // frozen dt sequence (adjoint forward) or null
+    double* dts_out;       // records the dt of every step, or null
+    int dts_cap;           // capacity of dts_in / dts_out
+    double fixed_dt;       // > 0: every step uses this dt (nest's rk2_step(dt))
+    int step_budget;       // resident 1D kernel: > 0 = at most this many steps per launch
+};
+
+// std::min / std::max semantics (first argument wins ties).
+template <typename T> __device__ __forceinline__ T smin(T a, T b) { return (b < a) ? b : a; }
+template <typename T> __device__ __forceinline__ T smax(T a, T b) { return (a < b) ? b : a; }
+
+__device__ __forceinline__ unsigned long long speed_bits(double s) {
+    return (unsigned long long)__double_as_longlong(s);
+}
+__device__ __forceinline__ double bits_speed(unsigned long long b) {
+    return __longlong_as_double((long long)b);
+}
+
+// Max over non-negative doubles: their IEEE bit patterns order like the values.
+__device__ __forceinline__ void atomic_max_speed(unsigned long long* slot, double s) {
+    atomicMax(slot, speed_bits(s));
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = smax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Decide the step: returns false when the run is finished.  Every block of
+// stage 1 evaluates this on the same inputs, so all agree; block 0 publishes.
+__device__ __forceinline__ bool step_is_done(const StepCtrl* c, int p, const LoopParams& lp) {
+    double t = c->time[p];
+    int s = c->step[p];
+    if (lp.t_final > 0.0 && !(t < lp.t_final)) return true;
+    if (lp.max_steps > 0 && s >= lp.max_steps) return true;
+    if (lp.dts_in && s >= lp.dts_cap) return true;
+    return false;
+}
+
+// dt of the step in slot p when it is not derived from the CFL condition:
+// a frozen sequence or a caller-given constant.  Returns a negative value
+// when the CFL rule applies.
+__device__ __forceinline__ double prescribed_dt(const StepCtrl* c, int p, const LoopParams& lp) {
+    if (lp.fixed_dt > 0.0) return lp.fixed_dt;
+    if (lp.dts_in) return lp.dts_in[c->step[p]];
+    return -1.0;
+}
+
+// Block 0 / thread 0 of stage 1: publish dt and prepare the next slot.
+__device__ __forceinline__ void publish_step(StepCtrl* c, int p, const LoopParams& lp, bool done, double dt) {
+    int q = p ^ 1;
+    if (done) {
+        c->active[p] = 0;
+        c->time[q] = c->time[p];
+        c->step[q] = c->step[p];
+        c->maxs[q][0] = c->maxs[p][0];
+        c->maxs[q][1] = c->maxs[p][1];
+        c->active[q] = 0;
+        return;
+    }
+    c->active[p] = 1;
+    c->dt[p] = dt;
+    c->time[q] = c->time[p] + dt;
+    c->step[q] = c->step[p] + 1;
+    c->maxs[q][0] = 0ull;
+    c->maxs[q][1] = 0ull;
+    int s = c->step[p];
+    if (lp.dts_out && s < lp.dts_cap) lp.dts_out[s] = dt;
+}
+
+// ---------------------------------------------------------------------------
+// 1D numerics (3 variables), examples/sod1d/euler1d.hpp
+// ---------------------------------------------------------------------------
+
+// eos_t::pressure, euler1d.hpp:31-44.
+__device__ __forceinline__ double eos_pressure(double gm1, double rho, double mom, double erg) {
+    double u = mom / rho;
+    double ke = 0.5 * rho * u * u;
+    double p = gm1 * (erg - ke);
+    return smax(p, 0.0);
+}
+
+// minmod, euler1d.hpp:112-115.
+template <typename T>
+__device__ __forceinline__ T minmod(T a, T b) {
+    if (a * b <= T(0)) return T(0);
+    return (fabs(a) < fabs(b)) ? a : b;
+}
+
+// hlle_flux, euler1d.hpp:178-242 (Davis speeds, three branches).
+__device__ __forceinline__ void hlle1d(double gamma, double gm1,
+                                       double rL, double uL, double pL,
+                                       double rR, double uR, double pR,
+                                       double& f0, double& f1, double& f2) {
+    double cL = sqrt(gamma * pL / rL);
+    double EL = pL / gm1 + 0.5 * rL * uL * uL;
+    double cR = sqrt(gamma * pR / rR);
+    double ER = pR / gm1 + 0.5 * rR * uR * uR;
+    double SL = smin(uL - cL, uR - cR);
+    double SR = smax(uL + cL, uR + cR);
+    double FL0 = rL * uL, FL1 = rL * uL * uL + pL, FL2 = (EL + pL) * uL;
+    double FR0 = rR * uR, FR1 = rR * uR * uR + pR, FR2 = (ER + pR) * uR;
+    if (SL >= 0.0) {
+        f0 = FL0; f1 = FL1; f2 = FL2;
+    } else if (SR <= 0.0) {
+        f0 = FR0; f1 = FR1; f2 = FR2;
+    } else {
+        double SLR = SL * SR, dS = SR - SL;
+        f0 = (SR * FL0 - SL * FR0 + SLR * (rR - rL)) / dS;
+        f1 = (SR * FL1 - SL * FR1 + SLR * (rR * uR - rL * uL)) / dS;
+        f2 = (SR * FL2 - SL * FR2 + SLR * (ER - EL)) / dS;
+    }
+}
+
+}  // namespace nestb

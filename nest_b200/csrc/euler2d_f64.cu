@@ -1,0 +1,58 @@
+// FP64 instantiation of the 2D stage kernels (the plain form).  Compiled with
+// -fmad=false and IEEE division / square root so that it reproduces the CPU
+// restatement of the scheme bit for bit.
+#include "euler2d_kernels.cuh"
+#include "kernels.h"
+
+namespace nestb {
+
+template <int STAGE>
+__global__ void __launch_bounds__(256) k2d_f64(StageArgs<double> a) {
+    stage2d_body<double, STAGE, false>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(256) k2d_prepare_f64(double* U, Geo2D g, StepCtrl* ctrl, int p) {
+    prepare2d_body<double>(U, g, ctrl, p);
+}
+
+cudaError_t launch_2d_prepare_f64(double* U, const Geo2D& g, StepCtrl* ctrl, int p, cudaStream_t st) {
+    dim3 b(32, 8), gr((g.ny + 4 + 31) / 32, (g.nx + 4 + 7) / 8);
+    k2d_prepare_f64<<<gr, b, 0, st>>>(U, g, ctrl, p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_2d_step_f64(double* U, double* U1, const Geo2D& g, const LoopParams& lp,
+                               StepCtrl* ctrl, double* partials, int p, int tx, int warps,
+                               int which, cudaStream_t st) {
+    int nstrips = (g.ny + STRIP - 1) / STRIP;
+    dim3 b(32, warps), gr((nstrips + warps - 1) / warps, (g.nx + tx - 1) / tx);
+    StageArgs<double> a1{U, nullptr, U1, g, lp, ctrl, nullptr, p, tx};
+    if (which & 1) k2d_f64<1><<<gr, b, 0, st>>>(a1);
+    StageArgs<double> a2{U1, U, U, g, lp, ctrl, partials, p, tx};
+    if (which & 2) k2d_f64<2><<<gr, b, 0, st>>>(a2);
+    return cudaGetLastError();
+}
+
+// Deterministic sum of per-warp totals: one block, fixed strided order, fixed tree.
+__global__ void __launch_bounds__(256) k_sum_partials(const double* part, long long nrec, double* out) {
+    __shared__ double s[4][256];
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (long long r = threadIdx.x; r < nrec; r += 256) {
+        a0 += part[4 * r]; a1 += part[4 * r + 1]; a2 += part[4 * r + 2]; a3 += part[4 * r + 3];
+    }
+    s[0][threadIdx.x] = a0; s[1][threadIdx.x] = a1; s[2][threadIdx.x] = a2; s[3][threadIdx.x] = a3;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int k = 0; k < 4; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) out[threadIdx.x] = s[threadIdx.x][0];
+}
+
+cudaError_t launch_sum_partials(const double* partials, long long nrec, double* out4, cudaStream_t st) {
+    k_sum_partials<<<1, 256, 0, st>>>(partials, nrec, out4);
+    return cudaGetLastError();
+}
+
+}  // namespace nestb

@@ -1,0 +1,35 @@
+// Internal launcher declarations shared by the kernel translation units and
+// the host runtime (capi.cpp).  Not part of the public C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "common.cuh"
+
+namespace nestb {
+
+struct Geo2D;
+
+// 1D (FP64, bit-exact with nest's OpenMP path)
+size_t resident_smem_bytes(int n, int h);
+cudaError_t launch_1d_resident(double* U, int n, int h, double dx, double gamma, int bc,
+                               const LoopParams& lp, StepCtrl* ctrl, int p, cudaStream_t st);
+cudaError_t launch_1d_prepare(double* U, int n, int h, double gamma, int bc, StepCtrl* ctrl, int p,
+                              cudaStream_t st);
+cudaError_t launch_1d_step(double* U, double* U1, int n, int h, double dx, double gamma, int bc,
+                           const LoopParams& lp, StepCtrl* ctrl, int p, int which, cudaStream_t st);
+
+// 2D unsplit scheme.  `which`: 1 = stage 1, 2 = stage 2, 3 = both.
+cudaError_t launch_2d_prepare_f64(double* U, const Geo2D& g, StepCtrl* ctrl, int p, cudaStream_t st);
+cudaError_t launch_2d_step_f64(double* U, double* U1, const Geo2D& g, const LoopParams& lp,
+                               StepCtrl* ctrl, double* partials, int p, int tx, int warps,
+                               int which, cudaStream_t st);
+cudaError_t launch_2d_prepare_f32(float* U, const Geo2D& g, StepCtrl* ctrl, int p, cudaStream_t st);
+cudaError_t launch_2d_step_f32(float* U, float* U1, const Geo2D& g, const LoopParams& lp,
+                               StepCtrl* ctrl, double* partials, int p, int tx, int warps,
+                               bool repair, int which, cudaStream_t st);
+// Fixed-order sum of per-warp totals (deterministic).
+cudaError_t launch_sum_partials(const double* partials, long long nrec, double* out4, cudaStream_t st);
+
+}  // namespace nestb

@@ -1,0 +1,92 @@
+"""1D FP64 path on the GPU against the oracle: bit for bit.
+
+Covers nest's drop-in ABI (euler1d_gpu_*), the resident single-CTA solver,
+the tiled multi-CTA path, periodic and outflow boundaries, ragged sizes,
+fixed-dt steps, compute_dt and frozen/recorded dt sequences."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle.oracle import BC_OUTFLOW, BC_PERIODIC, sod_ic_1d
+
+pytestmark = pytest.mark.gpu
+G = 1.4
+
+
+def test_dropin_matches_reference_test(gpu):
+    """nest's own CPU-vs-GPU test (tests/test_euler_cuda.cpp:280-306): it
+    allows 1e-8; the B200 path matches nest's CPU result exactly."""
+    want = np.load(GOLDEN / "sod100_periodic.npy")
+    s = gpu.Euler1DGPU(100, 2, 0.01, G)
+    s.upload(sod_ic_1d(100))
+    steps = s.run(0.1, 0.3)
+    got = s.download()
+    assert steps == 70
+    assert np.array_equal(got[:, 2:-2], want[:, 2:-2])
+
+
+@pytest.mark.parametrize("n,bc,cfl,tf", [(1024, BC_OUTFLOW, 0.4, 0.2), (1024, BC_PERIODIC, 0.4, 0.2),
+                                         (97, BC_OUTFLOW, 0.8, 0.1), (2300, BC_PERIODIC, 0.4, 0.05)])
+@pytest.mark.parametrize("resident", [True, False])
+def test_run_to_matches_oracle(gpu, oracle, n, bc, cfl, tf, resident):
+    U = sod_ic_1d(n)
+    want = U.copy()
+    wsteps, wt, _ = oracle.run1d(want, n, 2, 1.0 / n, G, cfl, t_final=tf, bc=bc)
+    s = gpu.Solver(1, n, bc=bc, flags=0 if resident else gpu.FLAG_NO_RESIDENT)
+    s.upload(U)
+    steps = s.run_to(tf, cfl)
+    t, total = s.time()
+    got = s.download()
+    assert steps == wsteps and total == wsteps and t == wt
+    assert np.array_equal(got[:, 2:-2], want[:, 2:-2])
+
+
+@pytest.mark.parametrize("n", [4, 255, 256, 257, 4099, 70001])
+def test_tiled_fixed_steps_ragged(gpu, oracle, n):
+    rng = np.random.default_rng(n)
+    x = np.arange(n + 4)
+    rho = 1.0 + 0.3 * np.sin(2 * np.pi * x / max(n, 8)) + 0.05 * rng.random(n + 4)
+    u = 0.2 * np.cos(2 * np.pi * x / max(n, 8))
+    p = 1.0 + 0.2 * rng.random(n + 4)
+    U = np.stack([rho, rho * u, p / 0.4 + 0.5 * rho * u * u])
+    want = U.copy()
+    oracle.run1d(want, n, 2, 1.0 / n, G, 0.5, nsteps=23, bc=BC_PERIODIC)
+    s = gpu.Solver(1, n, bc=BC_PERIODIC, flags=gpu.FLAG_NO_RESIDENT)
+    s.upload(U)
+    s.step(23, 0.5)
+    got = s.download()
+    assert np.array_equal(got[:, 2:-2], want[:, 2:-2])
+
+
+def test_compute_dt_and_rk2_step(gpu, oracle):
+    n = 300
+    U = sod_ic_1d(n)
+    s = gpu.Euler1DGPU(n, 2, 1.0 / n, G)
+    s.upload(U)
+    want = U.copy()
+    for _ in range(5):
+        dt = s.compute_dt(0.4)
+        assert dt == 0.4 * (1.0 / n) / oracle.max_speed1d(want, n, 2, G)
+        s.rk2_step(dt)
+        oracle.run1d(want, n, 2, 1.0 / n, G, 0.4, nsteps=1, bc=BC_PERIODIC, dts_in=np.array([dt]))
+    assert np.array_equal(s.download()[:, 2:-2], want[:, 2:-2])
+    ms, steps = s.run_timed(0.01, 0.4)
+    assert steps > 0 and ms > 0
+
+
+def test_dts_record_then_freeze(gpu):
+    n = 5000
+    s = gpu.Solver(1, n, bc=BC_OUTFLOW, flags=gpu.FLAG_NO_RESIDENT)
+    s.record_dts(64)
+    s.upload(sod_ic_1d(n))
+    s.step(40, 0.4)
+    dts = s.recorded_dts(40)
+    a = s.download()
+    s2 = gpu.Solver(1, n, bc=BC_OUTFLOW)
+    s2.freeze_dts(dts)
+    s2.upload(sod_ic_1d(n))
+    steps = s2.run_to(1.0, 0.4)  # ends when the frozen sequence runs out
+    assert steps == 40
+    assert np.array_equal(s2.download()[:, 2:-2], a[:, 2:-2])
