@@ -1,0 +1,408 @@
+"""Benchmark of the nest hot path on B200 (one JSON line on rank 0).
+
+Workload (default, --workload riemann2d): the 2D Euler Riemann problem on
+[0,1]^2 with 4096 x 4096 cells (16 x 16 patches of 256^2), outflow
+boundaries, CFL 0.4, gamma 1.4, 200 RK2 steps.  A bench step is one RK2 step
+of the whole grid (dt reduction, ghost fill, two fused stages).  Metric:
+cell-updates/s = interior cells x steps x 2 RK stages
+(examples/benchmark/benchmark_euler1d.cpp:217-218).  The headline form is
+FP32 (reconstruction, Riemann solve and update in FP32; FP64 dt/time); the
+FP64 plain form is measured in the same run.
+
+Arms
+  --impl ours       (default) the CUDA library through its C ABI.
+  --impl reference  the CPU implementation of the same scheme on the host
+                    cores (the oracle port: nest has no 2D RK2), one bounded
+                    sample per step.  Rank 0 only.
+
+Multi-GPU (torchrun): every rank advances its own copy of the workload
+(replicas; the single-domain path has no data-path collective here), timing
+is the max over ranks, value is the sum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-updates/s & %HBM roofline, FP32-batched vs FP64 plain; adjoint/fwd cost"
+UNIT = "cell-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["riemann2d"], default="riemann2d")
+    ap.add_argument("--n", type=int, default=4096, help="cells per axis")
+    ap.add_argument("--forms", default="f32,f64", help="forms to time; the first is the headline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    ap.add_argument("--tiling", default="", help="rows,warps: fixed launch shape instead of the tuned one")
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+
+def dist_setup():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(ws, x: float) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        import torch
+        ident = str(self.dev)
+        try:
+            pr = torch.cuda.get_device_properties(self.dev)
+            ident = "%08X:%02X:%02X.0" % (int(pr.pci_domain_id), int(pr.pci_bus_id), int(pr.pci_device_id))
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            if vis and vis.split(",")[self.dev].strip().isdigit():
+                ident = vis.split(",")[self.dev].strip()
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", ident, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append((time.time(), line.strip()))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, t0: float, t1: float):
+        if not self.rows:
+            return None
+        sel = [r for (t, r) in self.rows if t0 - 0.3 <= t <= t1 + 0.3] or [r for _, r in self.rows]
+        mhz, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in sel:
+            parts = [p.strip() for p in r.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                mhz.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not mhz:
+            return None
+        return {"sm_mhz": float(np.median(mhz)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def alg_bytes_per_cell(form: str):
+    """Algorithmic HBM bytes per cell of one launch: stage 1 reads U^n and
+    writes U1 (8 values); stage 2 reads U1 and U^n and writes U^{n+1}
+    (12 values).  Per cell-update that is 2.5 * 4 vars * s bytes."""
+    s = 4 if form == "f32" else 8
+    return {"stage1": 8 * s, "stage2": 12 * s, "per_cell_update": 10 * s}
+
+
+def traffic_from_profiles(form: str, n: int):
+    f = ROOT / "profiles" / "traffic.json"
+    if not f.exists():
+        return None
+    d = json.loads(f.read_text())
+    key = f"riemann2d_{form}"
+    if key not in d:
+        return None
+    e = d[key]
+    return {k: v * (n * n) / float(e["cells"]) for k, v in e["bytes_per_launch"].items()}
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import nest_b200 as nb
+    from nest_b200.problems import riemann_2d
+    from nest_b200.tuning import best_tiling
+
+    torch.cuda.set_device(local)
+    n = args.n
+    cells = n * n
+    cfl = 0.4
+    hbm, peak_kind = peaks()
+    st = torch.cuda.Stream()
+    U64 = riemann_2d(n, n)
+    results = {}
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    forms = [f.strip() for f in args.forms.split(",") if f.strip()]
+    launches = 0
+    for form in forms:
+        prec = nb.F32 if form == "f32" else nb.F64
+        U = U64.astype(np.float32) if form == "f32" else U64
+        s = nb.Solver(2, n, n, bc=nb.BC_OUTFLOW, precision=prec, stream=st.cuda_stream)
+        tiling = tuple(int(v) for v in args.tiling.split(",")) if args.tiling else best_tiling(form, n, n)
+        s.set_tiling(*tiling)
+        s.upload(U)
+        s.step(args.warmup, cfl)
+        s.sync()
+        # timed region: K steps from the initial state, one event between kernels
+        s.upload(U)
+        s.reset_time()
+        barrier(ws)
+        torch.cuda.synchronize()
+        t0 = time.time()
+        k1, k2, total = s.step_profiled(args.steps, cfl)
+        torch.cuda.synchronize()
+        t1 = time.time()
+        barrier(ws)
+        launches += 2 * args.steps
+        ms = allmax(ws, total) / args.steps
+        tsim, nst = s.time()
+        # the same K steps replayed through the captured CUDA graphs
+        s.upload(U)
+        s.reset_time()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        s.step(args.steps, cfl)
+        e1.record(st)
+        e1.synchronize()
+        graph_ms = e0.elapsed_time(e1) / args.steps
+        ab = alg_bytes_per_cell(form)
+        m1, m2 = float(np.mean(k1)), float(np.mean(k2))
+        dom, dom_ms = ("stage2", m2) if m2 >= m1 else ("stage1", m1)
+        achieved = ab[dom] * cells / (dom_ms * 1e-3) / 1e9
+        tr = traffic_from_profiles(form, n)
+        value = ws * cells * 2 * args.steps / (ms * args.steps * 1e-3)
+        results[form] = {
+            "value": value, "ms_per_step": ms, "graph_ms_per_step": graph_ms,
+            "sim_time": tsim, "steps": nst, "tiling": {"rows_per_tile": tiling[0], "warps_per_block": tiling[1]},
+            "kernel_ms": {"stage1": m1, "stage2": m2},
+            "hbm_gbs_step": value / ws * ab["per_cell_update"] / 1e9,
+            "roofline": {"bound": "hbm", "kernel": f"k2d_{form}<{dom[-1]}>", "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": ab[dom] * cells,
+                         "traffic": (tr or {}).get(dom)},
+            "window": (t0, t1),
+        }
+        if not args.no_e2e:
+            results[form]["e2e"] = e2e_run(s, U, args.steps, cfl, st, cells, ws)
+        s.close()
+        del s
+    clocks.stop()
+    head = forms[0]
+    r = results[head]
+    clk = clocks.summary(min(x["window"][0] for x in results.values()), max(x["window"][1] for x in results.values()))
+    for x in results.values():
+        x.pop("window")
+    out = {
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": head, "data": "synthetic",
+        "config": {"workload": f"riemann2d {n}x{n} {head}", "nx": n, "ny": n,
+                   "patches": f"{n // 256}x{n // 256} of 256^2" if n % 256 == 0 else "one",
+                   "bc": "outflow", "cfl": cfl, "gamma": 1.4, "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (two state buffers of %.0f MB each)" % (
+                       4 * (n + 4) ** 2 * (4 if head == "f32" else 8) / 1e6)},
+        "roofline": r["roofline"],
+        "forms": results,
+        "e2e": r.get("e2e"),
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    if ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(n, args.cpu_seconds)
+    return out
+
+
+def e2e_run(s, U, steps, cfl, st, cells, ws):
+    """Through the public API with pinned host buffers: upload the initial
+    state, run the K steps, download the final state and read the clock."""
+    import torch
+    import nest_b200 as nb
+    tdt = torch.float32 if U.dtype == np.float32 else torch.float64
+    hin = torch.empty(U.shape, dtype=tdt, pin_memory=True)
+    hin.numpy()[...] = U
+    hout = torch.empty(U.shape, dtype=tdt, pin_memory=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    nb.solver.check(nb._capi.lib.nest_solver_upload(s._h, hin.data_ptr(), nb.LAYOUT_EXTENDED), "upload")
+    s.reset_time()
+    s.step(steps, cfl)
+    nb.solver.check(nb._capi.lib.nest_solver_download(s._h, hout.data_ptr(), nb.LAYOUT_EXTENDED), "download")
+    t, k = s.time()
+    e1.record(st)
+    e1.synchronize()
+    ms = allmax(ws, e0.elapsed_time(e1))
+    nbytes = U.nbytes
+    return {"value": ws * cells * 2 * steps / (ms * 1e-3), "unit": UNIT, "ms_total": ms,
+            "h2d_bytes_per_step": nbytes / steps, "d2h_bytes_per_step": (nbytes + 32) / steps,
+            "api": "nest_solver_upload -> nest_solver_step -> nest_solver_download -> nest_solver_time"}
+
+
+# ---------------------------------------------------------------------------
+# CPU side (oracle port of the same scheme on the host cores)
+# ---------------------------------------------------------------------------
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(n: int, budget_s: float):
+    """FP64 scheme on the host cores: S RK2 steps of the full n x n problem,
+    S sized to about budget_s seconds of work."""
+    from oracle.oracle import BC_OUTFLOW, Oracle
+    from nest_b200.problems import riemann_2d
+    orc = Oracle()
+    th = host_threads()
+    orc.set_threads(th)
+    U = np.ascontiguousarray(riemann_2d(n, n))
+    t0 = time.perf_counter()
+    orc.run2d(U, n, n, 2, 1 / n, 1 / n, 1.4, 0.4, nsteps=1, bc=BC_OUTFLOW)
+    t1 = time.perf_counter() - t0
+    S = int(max(1, min(50, budget_s / max(t1, 1e-6) - 1)))
+    t0 = time.perf_counter()
+    orc.run2d(U, n, n, 2, 1 / n, 1 / n, 1.4, 0.4, nsteps=S, bc=BC_OUTFLOW)
+    el = time.perf_counter() - t0
+    return {"value": n * n * 2 * S / el, "unit": UNIT, "cores": th, "kind": "port",
+            "sample": f"{S} RK2 steps (after 1 untimed) of the {n}x{n} FP64 diagonal Riemann problem, "
+                      f"oracle/euler_oracle.c with OpenMP ({th} threads), {el:.1f} s"}
+
+
+def run_reference(args, rank):
+    """CPU arm: each step is one RK2 step of a sample of the workload -- the
+    first nx_s rows of the n x n grid as an outflow domain -- sized from the
+    warm-up timing so the whole run stays within minutes."""
+    from oracle.oracle import BC_OUTFLOW, Oracle
+    from nest_b200.problems import riemann_2d
+    orc = Oracle()
+    th = host_threads()
+    orc.set_threads(th)
+    n = args.n
+    nx_s = n
+    U = np.ascontiguousarray(riemann_2d(n, n))
+    t0 = time.perf_counter()
+    orc.run2d(U, n, n, 2, 1 / n, 1 / n, 1.4, 0.4, nsteps=1, bc=BC_OUTFLOW)
+    t1 = time.perf_counter() - t0
+    per_step_budget = 90.0 / max(1, args.steps + args.warmup)
+    if t1 > per_step_budget:
+        nx_s = max(64, int(n * per_step_budget / t1) // 64 * 64)
+    Us = np.ascontiguousarray(riemann_2d(n, n)[:, : nx_s + 4, :])
+    orc.run2d(Us, nx_s, n, 2, 1 / n, 1 / n, 1.4, 0.4, nsteps=max(1, args.warmup), bc=BC_OUTFLOW)
+    Us = np.ascontiguousarray(riemann_2d(n, n)[:, : nx_s + 4, :])
+    t0 = time.perf_counter()
+    orc.run2d(Us, nx_s, n, 2, 1 / n, 1 / n, 1.4, 0.4, nsteps=args.steps, bc=BC_OUTFLOW)
+    el = time.perf_counter() - t0
+    value = nx_s * n * 2 * args.steps / el
+    sample = (f"{args.steps} RK2 steps of a {nx_s}x{n} slab of the {n}x{n} FP64 diagonal Riemann problem, "
+              f"oracle/euler_oracle.c (the scheme's CPU restatement; nest has no 2D RK2), OpenMP {th} threads")
+    head = args.forms.split(",")[0].strip()
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"riemann2d {n}x{n} {head}", "nx": n, "ny": n, "bc": "outflow", "cfl": 0.4,
+                   "gamma": 1.4},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args, rank)), flush=True)
+        return 0
+    ws, rank, local = dist_setup()
+    out = run_ours(args, ws, rank, local)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

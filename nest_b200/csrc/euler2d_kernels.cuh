@@ -30,15 +30,23 @@ constexpr int STRIP = 28;  // output columns per warp
 
 template <typename T> struct Pol;
 
+// FP64 plain form: IEEE division and square root in nest's operation order.
 template <> struct Pol<double> {
+    static constexpr bool exact = true;
     __device__ static __forceinline__ double div(double a, double b) { return a / b; }
+    __device__ static __forceinline__ double rcp(double b) { return 1.0 / b; }
     __device__ static __forceinline__ double sound(double gamma, double p, double rho) { return sqrt(gamma * p / rho); }
 };
 
+// FP32 form: approximate reciprocal / reciprocal square root (one MUFU each).
 template <> struct Pol<float> {
+    static constexpr bool exact = false;
     __device__ static __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+    __device__ static __forceinline__ float rcp(float b) { return __fdividef(1.0f, b); }
+    // c = sqrt(g p / rho) = g p / sqrt(g p rho); the clamp keeps p = 0 finite (c = 0).
     __device__ static __forceinline__ float sound(float gamma, float p, float rho) {
-        return sqrtf(__fdividef(gamma * p, rho));
+        float gp = gamma * p;
+        return gp * rsqrtf(fmaxf(gp * rho, 1e-37f));
     }
 };
 
@@ -70,8 +78,14 @@ template <typename T, bool REPAIR>
 __device__ __forceinline__ Prim4<T> cons2prim(T U0, T U1, T U2, T U3, T gm1) {
     Prim4<T> w;
     w.r = U0;
-    w.u = Pol<T>::div(U1, U0);
-    w.v = Pol<T>::div(U2, U0);
+    if (Pol<T>::exact) {
+        w.u = Pol<T>::div(U1, U0);
+        w.v = Pol<T>::div(U2, U0);
+    } else {
+        T ir = Pol<T>::rcp(U0);
+        w.u = U1 * ir;
+        w.v = U2 * ir;
+    }
     T p = gm1 * (U3 - ke2(w.r, w.u, w.v));
     w.p = smax(p, T(0));
     if (REPAIR) {
@@ -90,28 +104,40 @@ __device__ __forceinline__ Prim4<T> cons2prim(T U0, T U1, T U2, T U3, T gm1) {
 // returns (rho un, rho un un + p, rho un ut, (E + p) un).  Operation order
 // and branches follow hlle_flux, euler1d.hpp:178-242.
 template <typename T>
-__device__ __forceinline__ void hlle4(T gamma, T gm1,
+__device__ __forceinline__ void hlle4(T gamma, T gm1, T igm1,
                                       T rL, T nL, T tL, T pL, T rR, T nR, T tR, T pR,
                                       T& f0, T& f1, T& f2, T& f3) {
     T cL = Pol<T>::sound(gamma, pL, rL);
     T cR = Pol<T>::sound(gamma, pR, rR);
-    T EL = Pol<T>::div(pL, gm1) + ke2(rL, nL, tL);
-    T ER = Pol<T>::div(pR, gm1) + ke2(rR, nR, tR);
+    T EL = (Pol<T>::exact ? Pol<T>::div(pL, gm1) : pL * igm1) + ke2(rL, nL, tL);
+    T ER = (Pol<T>::exact ? Pol<T>::div(pR, gm1) : pR * igm1) + ke2(rR, nR, tR);
     T SL = smin(nL - cL, nR - cR);
     T SR = smax(nL + cL, nR + cR);
     T mL = rL * nL, mR = rR * nR;
     T FL0 = mL, FL1 = mL * nL + pL, FL2 = mL * tL, FL3 = (EL + pL) * nL;
     T FR0 = mR, FR1 = mR * nR + pR, FR2 = mR * tR, FR3 = (ER + pR) * nR;
-    if (SL >= T(0)) {
-        f0 = FL0; f1 = FL1; f2 = FL2; f3 = FL3;
-    } else if (SR <= T(0)) {
-        f0 = FR0; f1 = FR1; f2 = FR2; f3 = FR3;
+    if (Pol<T>::exact) {
+        if (SL >= T(0)) {
+            f0 = FL0; f1 = FL1; f2 = FL2; f3 = FL3;
+        } else if (SR <= T(0)) {
+            f0 = FR0; f1 = FR1; f2 = FR2; f3 = FR3;
+        } else {
+            T SLR = SL * SR, dS = SR - SL;
+            f0 = Pol<T>::div(SR * FL0 - SL * FR0 + SLR * (rR - rL), dS);
+            f1 = Pol<T>::div(SR * FL1 - SL * FR1 + SLR * (mR - mL), dS);
+            f2 = Pol<T>::div(SR * FL2 - SL * FR2 + SLR * (rR * tR - rL * tL), dS);
+            f3 = Pol<T>::div(SR * FL3 - SL * FR3 + SLR * (ER - EL), dS);
+        }
     } else {
-        T SLR = SL * SR, dS = SR - SL;
-        f0 = Pol<T>::div(SR * FL0 - SL * FR0 + SLR * (rR - rL), dS);
-        f1 = Pol<T>::div(SR * FL1 - SL * FR1 + SLR * (mR - mL), dS);
-        f2 = Pol<T>::div(SR * FL2 - SL * FR2 + SLR * (rR * tR - rL * tL), dS);
-        f3 = Pol<T>::div(SR * FL3 - SL * FR3 + SLR * (ER - EL), dS);
+        // Branchless HLLE: with sl = min(SL, 0) and sr = max(SR, 0) the
+        // average formula reduces to F_L when SL >= 0 and to F_R when SR <= 0.
+        T sl = fmin(SL, T(0)), sr = fmax(SR, T(0));
+        T inv = Pol<T>::rcp(fmax(sr - sl, T(1e-30)));
+        T a = sr * inv, b = sl * inv, c = sl * sr * inv;
+        f0 = a * FL0 - b * FR0 + c * (rR - rL);
+        f1 = a * FL1 - b * FR1 + c * (mR - mL);
+        f2 = a * FL2 - b * FR2 + c * (rR * tR - rL * tL);
+        f3 = a * FL3 - b * FR3 + c * (ER - EL);
     }
 }
 
@@ -120,7 +146,15 @@ __device__ __forceinline__ void hlle4(T gamma, T gm1,
 template <typename T>
 __device__ __forceinline__ void cell_speeds(T U0, T U1, T U2, T U3, T gamma, T gm1, T& sx, T& sy) {
     T rho = smax(U0, T(1e-10));
-    T u = Pol<T>::div(U1, rho), v = Pol<T>::div(U2, rho);
+    T u, v;
+    if (Pol<T>::exact) {
+        u = Pol<T>::div(U1, rho);
+        v = Pol<T>::div(U2, rho);
+    } else {
+        T ir = Pol<T>::rcp(rho);
+        u = U1 * ir;
+        v = U2 * ir;
+    }
     T ke = T(0.5) * rho * (u * u + v * v);
     T p = smax(gm1 * (U3 - ke), T(1e-10));
     T c = Pol<T>::sound(gamma, p, rho);
@@ -137,9 +171,8 @@ __device__ __forceinline__ double dt_from_speeds(double sx, double sy, double dx
 }
 
 template <typename T>
-__device__ __forceinline__ void store_with_ghosts(T* Uo, const Geo2D& g, int k, int i, int j, T v) {
+__device__ __forceinline__ void store_ghosts(T* Uo, const Geo2D& g, int k, int i, int j, T v) {
     T* p = Uo + (long long)k * g.vstride;
-    p[g.at(i, j)] = v;
     if (g.bcy == BC_PERIODIC) {
         if (j < 2) p[g.at(i, j + g.ny)] = v;
         if (j >= g.ny - 2) p[g.at(i, j - g.ny)] = v;
@@ -201,6 +234,7 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
     const int lane = threadIdx.x & 31;
     const T gamma = (T)g.gamma;
     const T gm1 = (T)(g.gamma - 1.0);
+    const T igm1 = (T)(1.0 / (g.gamma - 1.0));
 
     double dt;
     if (STAGE == 1) {
@@ -260,7 +294,7 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
         if (r >= 1) {
             // x-face between rows r-2 and r-1 (normal u, transverse v)
             Win4<T> Fc;
-            hlle4<T>(gamma, gm1,
+            hlle4<T>(gamma, gm1, igm1,
                      W0.a + T(0.5) * S0.a, W0.b + T(0.5) * S0.b, W0.c + T(0.5) * S0.c, W0.d + T(0.5) * S0.d,
                      W1.a - T(0.5) * S1.a, W1.b - T(0.5) * S1.b, W1.c - T(0.5) * S1.c, W1.d - T(0.5) * S1.d,
                      Fc.a, Fc.b, Fc.c, Fc.d);
@@ -273,7 +307,7 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
                 Win4<T> Mq = { W0.a - T(0.5) * sy.a, W0.b - T(0.5) * sy.b, W0.c - T(0.5) * sy.c, W0.d - T(0.5) * sy.d };
                 Win4<T> Rq = shfl_dn4(Mq);
                 Win4<T> Gy;  // face j+1/2: normal v, transverse u
-                hlle4<T>(gamma, gm1,
+                hlle4<T>(gamma, gm1, igm1,
                          W0.a + T(0.5) * sy.a, W0.c + T(0.5) * sy.c, W0.b + T(0.5) * sy.b, W0.d + T(0.5) * sy.d,
                          Rq.a, Rq.c, Rq.b, Rq.d,
                          Gy.a, Gy.c, Gy.b, Gy.d);
@@ -310,10 +344,16 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
                         smy = smax(smy, (double)syv);
                         tot0 += (double)s0; tot1 += (double)s1; tot2 += (double)s2; tot3 += (double)s3;
                     }
-                    store_with_ghosts(a.Uout, g, 0, i, j, s0);
-                    store_with_ghosts(a.Uout, g, 1, i, j, s1);
-                    store_with_ghosts(a.Uout, g, 2, i, j, s2);
-                    store_with_ghosts(a.Uout, g, 3, i, j, s3);
+                    {
+                        long long o = g.at(i, j);
+                        a.Uout[o] = s0; a.Uout[vs + o] = s1; a.Uout[2 * vs + o] = s2; a.Uout[3 * vs + o] = s3;
+                    }
+                    if (i < 2 || i >= g.nx - 2 || j < 2 || j >= g.ny - 2) {
+                        store_ghosts(a.Uout, g, 0, i, j, s0);
+                        store_ghosts(a.Uout, g, 1, i, j, s1);
+                        store_ghosts(a.Uout, g, 2, i, j, s2);
+                        store_ghosts(a.Uout, g, 3, i, j, s3);
+                    }
                 }
             }
             Fp = Fc;
