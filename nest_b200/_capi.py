@@ -13,6 +13,7 @@ PKG = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("NEST_B200_LIB", PKG / "lib" / "libnest_b200.so"))
 
 NEST_OK = 0
+NEST_ERR_INVALID = 1
 STATUS_NAMES = {
     0: "NEST_OK", 1: "NEST_ERR_INVALID", 2: "NEST_ERR_CUDA", 3: "NEST_ERR_OOM",
     4: "NEST_ERR_NUMERIC", 5: "NEST_ERR_TIMEOUT", 6: "NEST_ERR_UNSUPPORTED",
@@ -81,7 +82,9 @@ _SIGS = {
     "nest_solver_set_dt_sequence": (_i, [_vp, _dp, _i, _i]),
     "nest_solver_get_dts": (_i, [_vp, _dp, _i]),
     "nest_solver_state_ptr": (_i, [_vp, C.POINTER(_vp), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "nest_euler1d_run_noalloc": (_i, [_vp, _i, _i, _d, _d, _i, _d, _d, _ip, _dp, _vp]),
 }
+NOALLOC_MAX_CELLS = 65552
 
 
 def bind(sigs: dict) -> None:

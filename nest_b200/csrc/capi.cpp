@@ -70,6 +70,8 @@ struct GraphKey {
 
 }  // namespace
 
+nest_status nestb::record_error(nest_status st, const std::string& msg) { return fail(st, msg); }
+
 struct nest_solver {
     nest_solver_desc d{};
     int h = 2;
@@ -450,6 +452,7 @@ nest_status nest_solver_run_to(nest_solver* s, double t_final, double cfl, int m
         if ((r = read_ctrl(s)) != NEST_OK) return r;
     } else {
         const int chunk = 4 * GRAPH_STEPS;
+        int last = -1;
         for (;;) {
             if ((r = enqueue_steps(s, chunk, lp)) != NEST_OK) return r;
             if ((r = read_ctrl(s)) != NEST_OK) return r;
@@ -458,6 +461,8 @@ nest_status nest_solver_run_to(nest_solver* s, double t_final, double cfl, int m
             if (!(c->time[p] < t_final)) break;
             if (lp.max_steps > 0 && c->step[p] >= lp.max_steps) break;
             if (s->dts_mode == 0 && c->step[p] >= s->dts_cap) break;
+            if (c->step[p] == last) return fail(NEST_ERR_NUMERIC, "time stopped advancing");
+            last = c->step[p];
         }
     }
     if (steps_out) *steps_out = s->host_ctrl->step[s->parity] - start;

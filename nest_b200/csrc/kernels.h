@@ -5,6 +5,10 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include <string>
+
+#include "../../include/nest_b200.h"
+
 #include "common.cuh"
 
 namespace nestb {
@@ -29,6 +33,9 @@ cudaError_t launch_2d_prepare_f32(float* U, const Geo2D& g, StepCtrl* ctrl, int 
 cudaError_t launch_2d_step_f32(float* U, float* U1, const Geo2D& g, const LoopParams& lp,
                                StepCtrl* ctrl, double* partials, int p, int tx, int warps,
                                bool repair, int which, cudaStream_t st);
+// Records msg as the calling thread's last error (read by nest_last_error()).
+nest_status record_error(nest_status st, const std::string& msg);
+
 // Fixed-order sum of per-warp totals (deterministic).
 cudaError_t launch_sum_partials(const double* partials, long long nrec, double* out4, cudaStream_t st);
 
