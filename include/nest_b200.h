@@ -143,6 +143,31 @@ nest_status nest_solver_get_dts(nest_solver* s, double* dts, int n);
 /* Device state: base pointer, row pitch (elements) and plane stride (elements). */
 nest_status nest_solver_state_ptr(nest_solver* s, void** dev, long long* pitch, long long* vstride);
 
+/* ------------------------------------------------------------------------ */
+/* Allocation-free 1D run.  No counterpart in nest's ABI.                   */
+/*                                                                          */
+/* For callers that cannot allocate device memory (a host code that owns    */
+/* the whole GPU through its own pool, a plugin host that forbids library   */
+/* allocations, a real-time loop that must not allocate after start-up).    */
+/* The caller passes the state; the solver's scratch (stage buffer and      */
+/* control block) is a fixed array inside the library, so this call makes   */
+/* no cudaMalloc / cudaFree.  The array holds n_interior + 2*n_halo <=      */
+/* NEST_NOALLOC_MAX_CELLS cells (about 1.6 MB, held by every GPU that loads */
+/* the library until exit); larger sizes return NEST_ERR_INVALID.  The      */
+/* first call on a device looks up the array's device address, so make it   */
+/* before any stream capture.  All calls share the array: calls that        */
+/* overlap on the GPU race.                                                 */
+/*                                                                          */
+/* d_state: device SoA [var * n_total + i], n_total = n_interior + 2 n_halo */
+/* (nest's layout), advanced in place from time 0 to t_final with CFL dt,   */
+/* periodic or outflow boundaries, on `stream` (NULL: legacy stream); waits */
+/* for the result.  Same arithmetic as euler1d_gpu_run (bit for bit).       */
+/* ------------------------------------------------------------------------ */
+#define NEST_NOALLOC_MAX_CELLS 65552
+nest_status nest_euler1d_run_noalloc(double* d_state, int n_interior, int n_halo, double dx, double gamma,
+                                     int bc, double t_final, double cfl, int* steps_out, double* time_out,
+                                     void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,6 +29,7 @@ UNITS = {
     "euler2d_f64.cu": ["-fmad=false"],
     "euler2d_f32.cu": ["-use_fast_math"],
     "capi.cpp": ["-x", "cu"],
+    "noalloc.cu": [],
 }
 
 
