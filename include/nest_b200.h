@@ -49,7 +49,8 @@ enum { NEST_LAYOUT_EXTENDED = 0, NEST_LAYOUT_INTERIOR = 1 };
 enum {
     NEST_FLAG_TOTALS = 1,       /* keep FP64 conserved totals each step (2D) */
     NEST_FLAG_REPAIR = 2,       /* FP32 form: FP64 positivity repair near vacuum */
-    NEST_FLAG_NO_RESIDENT = 4   /* 1D: never use the single-CTA resident solver */
+    NEST_FLAG_NO_RESIDENT = 4,  /* 1D: never use the single-CTA resident solver */
+    NEST_FLAG_FP32_SCALAR = 8   /* FP32 form: one column per lane instead of packed FP32x2 pairs */
 };
 
 /* ------------------------------------------------------------------------ */

@@ -151,8 +151,11 @@ cudaError_t enqueue_step(nest_solver* s, const LoopParams& lp, int p, int which 
     if (s->d.precision == NEST_F64)
         return launch_2d_step_f64((double*)s->U, (double*)s->U1, s->geo(), lp, s->ctrl, s->partials, p, s->tx,
                                   s->warps, which, s->st);
-    return launch_2d_step_f32((float*)s->U, (float*)s->U1, s->geo(), lp, s->ctrl, s->partials, p, s->tx, s->warps,
-                              (s->d.flags & NEST_FLAG_REPAIR) != 0, which, s->st);
+    if (s->d.flags & NEST_FLAG_FP32_SCALAR)
+        return launch_2d_step_f32((float*)s->U, (float*)s->U1, s->geo(), lp, s->ctrl, s->partials, p, s->tx,
+                                  s->warps, (s->d.flags & NEST_FLAG_REPAIR) != 0, which, s->st);
+    return launch_2d_step_f32x2((float*)s->U, (float*)s->U1, s->geo(), lp, s->ctrl, s->partials, p, s->tx,
+                                s->warps, (s->d.flags & NEST_FLAG_REPAIR) != 0, which, s->st);
 }
 
 // Enqueue nsteps steps of the tiled path; whole chunks go through cached graphs.

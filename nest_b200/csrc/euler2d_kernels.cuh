@@ -275,8 +275,8 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
 
     // Window: rows r-2, r-1, r (W0, W1, W2); slopes of rows r-2, r-1 (S0, S1);
     // conserved values of rows r-2, r-1, r (C0, C1, C2); x-flux of face (r-3)+1/2.
-    Win4<T> W0, W1, W2, S0, S1, C0, C1, C2, Fp;
-    Win4<T> nxt;
+    Win4<T> W0, W1, W2, S0, S1, Fp;
+    Win4<T> nxt, C0, N0;
     double smx = 0.0, smy = 0.0;
     double tot0 = 0.0, tot1 = 0.0, tot2 = 0.0, tot3 = 0.0;
 
@@ -284,9 +284,18 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
     for (int r = -2; r <= rows + 1; ++r) {
         Win4<T> cur = nxt;
         if (r + 1 <= rows + 1) load(i0 + r + 1, nxt.a, nxt.b, nxt.c, nxt.d);
+        if (r >= 2) {
+            // conserved values of the row to update (an L1 hit: loaded as
+            // `cur` two iterations ago) and, for stage 2, its U^n, requested
+            // ahead of this iteration's flux work
+            load(i0 + r - 2, C0.a, C0.b, C0.c, C0.d);
+            if (STAGE == 2) {
+                long long o = g.at(i0 + r - 2, jc);
+                N0.a = a.Un[o]; N0.b = a.Un[vs + o]; N0.c = a.Un[2 * vs + o]; N0.d = a.Un[3 * vs + o];
+            }
+        }
         Prim4<T> w = cons2prim<T, REPAIR>(cur.a, cur.b, cur.c, cur.d, gm1);
         W0 = W1; W1 = W2; W2 = prim_win(w);
-        C0 = C1; C1 = C2; C2 = cur;
         if (r >= 0) {
             S0 = S1;
             S1 = minmod4(W0, W1, W2);  // slope of row r-1
@@ -318,11 +327,10 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
                     T s2 = C0.c - (dtdx * (Fc.c - Fp.c) + dtdy * (Gy.c - Gl.c));
                     T s3 = C0.d - (dtdx * (Fc.d - Fp.d) + dtdy * (Gy.d - Gl.d));
                     if (STAGE == 2) {
-                        long long o = g.at(i, j);
-                        s0 = T(0.5) * (a.Un[o] + s0);
-                        s1 = T(0.5) * (a.Un[vs + o] + s1);
-                        s2 = T(0.5) * (a.Un[2 * vs + o] + s2);
-                        s3 = T(0.5) * (a.Un[3 * vs + o] + s3);
+                        s0 = T(0.5) * (N0.a + s0);
+                        s1 = T(0.5) * (N0.b + s1);
+                        s2 = T(0.5) * (N0.c + s2);
+                        s3 = T(0.5) * (N0.d + s3);
                         if (REPAIR) {
                             // positivity repair of the new state in FP64
                             const double fl = 1e-10;

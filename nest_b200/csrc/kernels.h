@@ -33,6 +33,12 @@ cudaError_t launch_2d_prepare_f32(float* U, const Geo2D& g, StepCtrl* ctrl, int 
 cudaError_t launch_2d_step_f32(float* U, float* U1, const Geo2D& g, const LoopParams& lp,
                                StepCtrl* ctrl, double* partials, int p, int tx, int warps,
                                bool repair, int which, cudaStream_t st);
+// FP32 form with packed FP32x2 arithmetic, two columns per lane (60 output
+// columns per warp).
+cudaError_t launch_2d_step_f32x2(float* U, float* U1, const Geo2D& g, const LoopParams& lp, StepCtrl* ctrl,
+                                 double* partials, int p, int tx, int warps, bool repair, int which,
+                                 cudaStream_t st);
+
 // Records msg as the calling thread's last error (read by nest_last_error()).
 nest_status record_error(nest_status st, const std::string& msg);
 
