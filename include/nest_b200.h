@@ -145,6 +145,47 @@ nest_status nest_solver_get_dts(nest_solver* s, double* dts, int n);
 nest_status nest_solver_state_ptr(nest_solver* s, void** dev, long long* pitch, long long* vstride);
 
 /* ------------------------------------------------------------------------ */
+/* Batched independent 2D problems (uneven sizes).  One persistent launch   */
+/* per stage walks a device work list of (problem, column strip, row tile); */
+/* each problem keeps its own dt, time and FP64 totals; runs of steps are   */
+/* captured into CUDA graphs.  No counterpart in nest (its patches are      */
+/* advanced by serial host loops, examples/sod2d/sod2d.cpp:318-366).        */
+/* ------------------------------------------------------------------------ */
+
+typedef struct nest_batch nest_batch;
+
+typedef struct nest_batch_desc {
+    int count;            /* number of problems */
+    const int* nx;        /* [count] interior cells along x */
+    const int* ny;        /* [count] interior cells along y */
+    const double* dx;     /* [count] or NULL: 1/nx */
+    const double* dy;     /* [count] or NULL: 1/ny */
+    double gamma;
+    int bc_x, bc_y;       /* NEST_BC_*, shared by all problems */
+    int precision;        /* NEST_F64 (bit-exact per problem) or NEST_F32 (packed FP32x2) */
+    int flags;            /* NEST_FLAG_TOTALS, NEST_FLAG_REPAIR */
+    void* stream;
+} nest_batch_desc;
+
+nest_status nest_batch_create(const nest_batch_desc* desc, nest_batch** out);
+nest_status nest_batch_destroy(nest_batch* b);
+/* One problem's state, in the batch precision and the solver layouts. */
+nest_status nest_batch_upload(nest_batch* b, int problem, const void* host, int layout);
+nest_status nest_batch_download(nest_batch* b, int problem, void* host, int layout);
+/* Enqueue nsteps steps of every problem (CFL dt per problem); returns without waiting. */
+nest_status nest_batch_step(nest_batch* b, int nsteps, double cfl);
+/* As nest_batch_step with a CUDA event between kernels; waits (see nest_solver_step_profiled). */
+nest_status nest_batch_step_profiled(nest_batch* b, int nsteps, double cfl, float* stage_ms, float* total_ms);
+/* Per-problem simulated time and step count (waits). */
+nest_status nest_batch_times(nest_batch* b, double* times, int* steps);
+/* Per-problem FP64 totals [count][4] after the last step (needs NEST_FLAG_TOTALS). */
+nest_status nest_batch_totals(nest_batch* b, double* out);
+/* Launch shape: rows per work item, warps per block, blocks per SM (0 = occupancy limit). */
+nest_status nest_batch_set_tiling(nest_batch* b, int rows_per_tile, int warps_per_block, int blocks_per_sm);
+/* Total interior cells, work items and persistent blocks. */
+nest_status nest_batch_info(nest_batch* b, long long* cells, int* items, int* blocks);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free 1D run.  No counterpart in nest's ABI.                   */
 /*                                                                          */
 /* For callers that cannot allocate device memory (a host code that owns    */

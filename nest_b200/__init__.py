@@ -6,10 +6,11 @@ fallback.
 """
 from ._capi import (BC_OUTFLOW, BC_PERIODIC, F32, F64, FLAG_FP32_SCALAR, FLAG_NO_RESIDENT, FLAG_REPAIR,
                     FLAG_TOTALS, LAYOUT_EXTENDED, LAYOUT_INTERIOR, LIB_PATH, NestError)
+from .batch import Batch
 from .solver import Euler1DGPU, Solver
 
 __all__ = [
-    "Euler1DGPU", "Solver", "NestError", "BC_PERIODIC", "BC_OUTFLOW", "F64", "F32",
+    "Batch", "Euler1DGPU", "Solver", "NestError", "BC_PERIODIC", "BC_OUTFLOW", "F64", "F32",
     "LAYOUT_EXTENDED", "LAYOUT_INTERIOR", "FLAG_TOTALS", "FLAG_REPAIR", "FLAG_NO_RESIDENT", "FLAG_FP32_SCALAR",
     "LIB_PATH",
 ]

@@ -18,6 +18,7 @@
 #include <new>
 #include <string>
 #include <tuple>
+#include <vector>
 
 #include "../../include/nest_b200.h"
 #include "common.cuh"
@@ -682,6 +683,348 @@ nest_status euler1d_gpu_set_bc(euler1d_gpu_t* h, int bc) {
 nest_status euler1d_gpu_status(euler1d_gpu_t* h) {
     if (!h) return NEST_ERR_INVALID;
     return h->last;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched independent 2D problems
+// ===========================================================================
+
+struct nest_batch {
+    nest_batch_desc d{};
+    int count = 0;
+    std::vector<BatchProblem> probs;      // host copy
+    std::vector<int> first;               // first item of each problem (+ total)
+    std::vector<int4> items;
+    size_t esize = 4;
+    long long total_elems = 0;
+    void* U = nullptr;
+    void* U1 = nullptr;
+    BatchProblem* dprobs = nullptr;
+    int4* ditems = nullptr;
+    int* dfirst = nullptr;
+    StepCtrl* ctrls = nullptr;
+    StepCtrl* host_ctrls = nullptr;
+    double* partials = nullptr;
+    double* totals_dev = nullptr;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    int parity = 0;
+    bool prepared = false;
+    int tx = 32, warps = 2, blocks = 0;
+    std::map<GraphKey, cudaGraphExec_t> graphs;
+    int strip_w() const { return d.precision == NEST_F64 ? STRIP : 60; }
+};
+
+namespace {
+
+nest_status batch_build_items(nest_batch* b) {
+    b->items.clear();
+    b->first.assign(b->count + 1, 0);
+    int sw = b->strip_w();
+    for (int p = 0; p < b->count; ++p) {
+        const Geo2D& g = b->probs[p].g;
+        int nstrips = (g.ny + sw - 1) / sw, ntiles = (g.nx + b->tx - 1) / b->tx;
+        b->first[p] = (int)b->items.size();
+        b->probs[p].item0 = b->first[p];
+        for (int t = 0; t < ntiles; ++t)
+            for (int sidx = 0; sidx < nstrips; ++sidx) b->items.push_back(make_int4(p, sidx, t, 0));
+    }
+    b->first[b->count] = (int)b->items.size();
+    cudaFree(b->ditems); b->ditems = nullptr;
+    cudaFree(b->dfirst); b->dfirst = nullptr;
+    cudaFree(b->partials); b->partials = nullptr;
+    CK(cudaMalloc(&b->ditems, sizeof(int4) * b->items.size()));
+    CK(cudaMalloc(&b->dfirst, sizeof(int) * (b->count + 1)));
+    CK(cudaMemcpy(b->ditems, b->items.data(), sizeof(int4) * b->items.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->dfirst, b->first.data(), sizeof(int) * (b->count + 1), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->dprobs, b->probs.data(), sizeof(BatchProblem) * b->count, cudaMemcpyHostToDevice));
+    if (b->d.flags & NEST_FLAG_TOTALS) {
+        CK(cudaMalloc(&b->partials, sizeof(double) * 4 * b->items.size()));
+        CK(cudaMemset(b->partials, 0, sizeof(double) * 4 * b->items.size()));
+    }
+    for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    b->graphs.clear();
+    return NEST_OK;
+}
+
+template <typename T>
+BatchArgs<T> batch_args(nest_batch* b, const LoopParams& lp, int p) {
+    BatchArgs<T> a;
+    a.U = (T*)b->U; a.U1 = (T*)b->U1; a.probs = b->dprobs; a.items = b->ditems; a.nitems = (int)b->items.size();
+    a.ctrls = b->ctrls; a.partials = b->partials; a.lp = lp; a.p = p; a.tx = b->tx;
+    return a;
+}
+
+cudaError_t batch_enqueue_step(nest_batch* b, const LoopParams& lp, int p, int which = 3) {
+    if (b->d.precision == NEST_F64)
+        return launch_batch_f64(batch_args<double>(b, lp, p), which, b->blocks, b->warps, b->st);
+    return launch_batch_f32x2(batch_args<float>(b, lp, p), (b->d.flags & NEST_FLAG_REPAIR) != 0, which,
+                              b->blocks, b->warps, b->st);
+}
+
+nest_status batch_prepare(nest_batch* b) {
+    for (int p = 0; p < b->count; ++p) {
+        CK(cudaMemsetAsync(&b->ctrls[p].maxs[b->parity][0], 0, 2 * sizeof(unsigned long long), b->st));
+        cudaError_t e;
+        if (b->d.precision == NEST_F64)
+            e = launch_2d_prepare_f64((double*)b->U + b->probs[p].off, b->probs[p].g, b->ctrls + p, b->parity, b->st);
+        else
+            e = launch_2d_prepare_f32((float*)b->U + b->probs[p].off, b->probs[p].g, b->ctrls + p, b->parity, b->st);
+        if (e != cudaSuccess) return cuda_fail(e, "batch prepare");
+    }
+    b->prepared = true;
+    return NEST_OK;
+}
+
+nest_status batch_check(const nest_batch* b) {
+    if (!b) return fail(NEST_ERR_INVALID, "null batch handle");
+    return NEST_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nest_status nest_batch_create(const nest_batch_desc* d, nest_batch** out) {
+    if (!d || !out || !d->nx || !d->ny) return fail(NEST_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (d->count <= 0) return fail(NEST_ERR_INVALID, "count must be positive");
+    if (d->precision != NEST_F64 && d->precision != NEST_F32) return fail(NEST_ERR_INVALID, "bad precision");
+    if (!(d->gamma > 1.0)) return fail(NEST_ERR_INVALID, "gamma must exceed 1");
+    if (d->bc_x != NEST_BC_PERIODIC && d->bc_x != NEST_BC_OUTFLOW) return fail(NEST_ERR_INVALID, "bad bc_x");
+    if (d->bc_y != NEST_BC_PERIODIC && d->bc_y != NEST_BC_OUTFLOW) return fail(NEST_ERR_INVALID, "bad bc_y");
+    for (int p = 0; p < d->count; ++p)
+        if (d->nx[p] < 4 || d->ny[p] < 4) return fail(NEST_ERR_INVALID, "every problem needs >= 4 cells per axis");
+    nest_batch* b = new (std::nothrow) nest_batch;
+    if (!b) return fail(NEST_ERR_OOM, "host allocation failed");
+    b->d = *d;
+    b->count = d->count;
+    b->esize = d->precision == NEST_F64 ? 8 : 4;
+    auto cleanup = [&](nest_status st) { nest_batch_destroy(b); return st; };
+    b->probs.resize(b->count);
+    long long off = 0;
+    int align = (int)(128 / b->esize);
+    long long pad = 256 / (long long)b->esize;
+    for (int p = 0; p < b->count; ++p) {
+        Geo2D g;
+        g.nx = d->nx[p]; g.ny = d->ny[p];
+        g.pitch = ((g.ny + 4 + align - 1) / align) * align;
+        g.vstride = (((long long)g.pitch * (g.nx + 4)) + pad - 1) / pad * pad;
+        g.bcx = d->bc_x; g.bcy = d->bc_y;
+        g.dx = d->dx ? d->dx[p] : 1.0 / g.nx;
+        g.dy = d->dy ? d->dy[p] : 1.0 / g.ny;
+        g.gamma = d->gamma;
+        b->probs[p].g = g;
+        b->probs[p].off = off;
+        off += 4 * g.vstride;
+    }
+    b->total_elems = off;
+    cudaError_t e;
+    if (d->stream) {
+        b->st = (cudaStream_t)d->stream;
+    } else {
+        if ((e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking)) != cudaSuccess)
+            return cleanup(cuda_fail(e, "cudaStreamCreate"));
+        b->own_stream = true;
+    }
+    size_t bytes = b->esize * (size_t)off;
+    if ((e = cudaMalloc(&b->U, bytes)) != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(U)"));
+    if ((e = cudaMalloc(&b->U1, bytes)) != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(U1)"));
+    if ((e = cudaMemset(b->U, 0, bytes)) != cudaSuccess) return cleanup(cuda_fail(e, "memset"));
+    if ((e = cudaMemset(b->U1, 0, bytes)) != cudaSuccess) return cleanup(cuda_fail(e, "memset"));
+    if ((e = cudaMalloc(&b->dprobs, sizeof(BatchProblem) * b->count)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "cudaMalloc(probs)"));
+    if ((e = cudaMalloc(&b->ctrls, sizeof(StepCtrl) * b->count)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "cudaMalloc(ctrls)"));
+    if ((e = cudaMemset(b->ctrls, 0, sizeof(StepCtrl) * b->count)) != cudaSuccess) return cleanup(cuda_fail(e, "memset"));
+    if ((e = cudaMallocHost(&b->host_ctrls, sizeof(StepCtrl) * b->count)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "cudaMallocHost"));
+    if ((e = cudaMalloc(&b->totals_dev, sizeof(double) * 4 * b->count)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "cudaMalloc(totals)"));
+    int sms = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = d->precision == NEST_F64 ? batch_max_blocks_f64(b->warps) : batch_max_blocks_f32x2(b->warps);
+    b->blocks = sms * (per_sm > 0 ? per_sm : 1);
+    nest_status r = batch_build_items(b);
+    if (r != NEST_OK) return cleanup(r);
+    *out = b;
+    return NEST_OK;
+}
+
+nest_status nest_batch_destroy(nest_batch* b) {
+    if (!b) return NEST_OK;
+    if (b->st) cudaStreamSynchronize(b->st);
+    for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    cudaFree(b->U); cudaFree(b->U1); cudaFree(b->dprobs); cudaFree(b->ditems); cudaFree(b->dfirst);
+    cudaFree(b->ctrls); cudaFree(b->partials); cudaFree(b->totals_dev);
+    if (b->host_ctrls) cudaFreeHost(b->host_ctrls);
+    if (b->own_stream && b->st) cudaStreamDestroy(b->st);
+    delete b;
+    return NEST_OK;
+}
+
+static nest_status batch_copy(nest_batch* b, int p, void* dst, const void* src, int layout, bool up) {
+    if (p < 0 || p >= b->count) return fail(NEST_ERR_INVALID, "problem index out of range");
+    if (layout != NEST_LAYOUT_EXTENDED && layout != NEST_LAYOUT_INTERIOR) return fail(NEST_ERR_INVALID, "bad layout");
+    const Geo2D& g = b->probs[p].g;
+    size_t es = b->esize;
+    int rows = layout == NEST_LAYOUT_EXTENDED ? g.nx + 4 : g.nx;
+    int cols = layout == NEST_LAYOUT_EXTENDED ? g.ny + 4 : g.ny;
+    size_t off = layout == NEST_LAYOUT_EXTENDED ? 0 : (size_t)(2 * g.pitch + 2);
+    for (int k = 0; k < 4; ++k) {
+        char* dev = (char*)b->U + es * (b->probs[p].off + (size_t)k * g.vstride + off);
+        size_t hoff = es * (size_t)k * rows * cols;
+        if (up)
+            CK(cudaMemcpy2DAsync(dev, es * g.pitch, (const char*)src + hoff, es * cols, es * cols, rows,
+                                 cudaMemcpyDefault, b->st));
+        else
+            CK(cudaMemcpy2DAsync((char*)dst + hoff, es * cols, dev, es * g.pitch, es * cols, rows,
+                                 cudaMemcpyDefault, b->st));
+    }
+    CK(cudaStreamSynchronize(b->st));
+    return NEST_OK;
+}
+
+nest_status nest_batch_upload(nest_batch* b, int problem, const void* host, int layout) {
+    nest_status r = batch_check(b);
+    if (r != NEST_OK) return r;
+    if (!host) return fail(NEST_ERR_INVALID, "null source");
+    b->prepared = false;
+    return batch_copy(b, problem, nullptr, host, layout, true);
+}
+
+nest_status nest_batch_download(nest_batch* b, int problem, void* host, int layout) {
+    nest_status r = batch_check(b);
+    if (r != NEST_OK) return r;
+    if (!host) return fail(NEST_ERR_INVALID, "null destination");
+    return batch_copy(b, problem, host, nullptr, layout, false);
+}
+
+nest_status nest_batch_set_tiling(nest_batch* b, int rows_per_tile, int warps_per_block, int blocks_per_sm) {
+    nest_status r = batch_check(b);
+    if (r != NEST_OK) return r;
+    if (rows_per_tile < 8 || rows_per_tile > 4096) return fail(NEST_ERR_INVALID, "rows per tile must be in [8, 4096]");
+    if (warps_per_block < 1 || warps_per_block > 8) return fail(NEST_ERR_INVALID, "warps per block must be in [1, 8]");
+    CK(cudaStreamSynchronize(b->st));
+    b->tx = rows_per_tile;
+    b->warps = warps_per_block;
+    int sms = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = b->d.precision == NEST_F64 ? batch_max_blocks_f64(b->warps) : batch_max_blocks_f32x2(b->warps);
+    if (per_sm < 1) per_sm = 1;
+    if (blocks_per_sm > 0 && blocks_per_sm < per_sm) per_sm = blocks_per_sm;
+    b->blocks = sms * per_sm;
+    return batch_build_items(b);
+}
+
+nest_status nest_batch_step(nest_batch* b, int nsteps, double cfl) {
+    nest_status r = batch_check(b);
+    if (r != NEST_OK) return r;
+    if (nsteps < 0 || !(cfl > 0.0)) return fail(NEST_ERR_INVALID, "need nsteps >= 0 and cfl > 0");
+    if (!b->prepared && (r = batch_prepare(b)) != NEST_OK) return r;
+    LoopParams lp{};
+    lp.cfl = cfl;
+    while (nsteps > 0) {
+        if (nsteps >= GRAPH_STEPS) {
+            GraphKey k{GRAPH_STEPS, b->parity, cfl, 0.0, 0.0, 0, nullptr, nullptr, 0, b->tx, b->warps * 1000 + b->blocks};
+            auto it = b->graphs.find(k);
+            if (it == b->graphs.end()) {
+                cudaGraph_t g;
+                CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+                int p = b->parity;
+                cudaError_t e = cudaSuccess;
+                for (int i = 0; i < GRAPH_STEPS && e == cudaSuccess; ++i, p ^= 1) e = batch_enqueue_step(b, lp, p);
+                cudaError_t e2 = cudaStreamEndCapture(b->st, &g);
+                if (e != cudaSuccess) return cuda_fail(e, "batch capture");
+                if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+                cudaGraphExec_t ge;
+                cudaError_t e3 = cudaGraphInstantiate(&ge, g, 0);
+                cudaGraphDestroy(g);
+                if (e3 != cudaSuccess) return cuda_fail(e3, "cudaGraphInstantiate");
+                it = b->graphs.emplace(k, ge).first;
+            }
+            CK(cudaGraphLaunch(it->second, b->st));
+            nsteps -= GRAPH_STEPS;
+        } else {
+            cudaError_t e = batch_enqueue_step(b, lp, b->parity);
+            if (e != cudaSuccess) return cuda_fail(e, "batch step");
+            b->parity ^= 1;
+            --nsteps;
+        }
+    }
+    return NEST_OK;
+}
+
+nest_status nest_batch_step_profiled(nest_batch* b, int nsteps, double cfl, float* stage_ms, float* total_ms) {
+    nest_status r = batch_check(b);
+    if (r != NEST_OK) return r;
+    if (nsteps <= 0 || !(cfl > 0.0)) return fail(NEST_ERR_INVALID, "need nsteps > 0 and cfl > 0");
+    if (!b->prepared && (r = batch_prepare(b)) != NEST_OK) return r;
+    LoopParams lp{};
+    lp.cfl = cfl;
+    std::vector<cudaEvent_t> ev(2 * nsteps + 1);
+    int made = 0;
+    cudaError_t e = cudaSuccess;
+    for (; made < (int)ev.size() && e == cudaSuccess; ++made) e = cudaEventCreate(&ev[made]);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[0], b->st);
+    for (int i = 0; i < nsteps && e == cudaSuccess; ++i) {
+        e = batch_enqueue_step(b, lp, b->parity, 1);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[2 * i + 1], b->st);
+        if (e == cudaSuccess) e = batch_enqueue_step(b, lp, b->parity, 2);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[2 * i + 2], b->st);
+        b->parity ^= 1;
+    }
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev.back());
+    for (int i = 0; i < 2 * nsteps && e == cudaSuccess; ++i) {
+        float ms = 0.f;
+        e = cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+        if (stage_ms) stage_ms[i] = ms;
+    }
+    if (e == cudaSuccess && total_ms) e = cudaEventElapsedTime(total_ms, ev[0], ev.back());
+    for (int i = 0; i < made; ++i) cudaEventDestroy(ev[i]);
+    if (e != cudaSuccess) return cuda_fail(e, "profiled batch steps");
+    return NEST_OK;
+}
+
+nest_status nest_batch_times(nest_batch* b, double* times, int* steps) {
+    nest_status r = batch_check(b);
+    if (r != NEST_OK) return r;
+    CK(cudaMemcpyAsync(b->host_ctrls, b->ctrls, sizeof(StepCtrl) * b->count, cudaMemcpyDeviceToHost, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    for (int p = 0; p < b->count; ++p) {
+        if (b->host_ctrls[p].err & ERRW_NONFINITE) return fail(NEST_ERR_NUMERIC, "non-finite wave speed in problem " + std::to_string(p));
+        if (times) times[p] = b->host_ctrls[p].time[b->parity];
+        if (steps) steps[p] = b->host_ctrls[p].step[b->parity];
+    }
+    return NEST_OK;
+}
+
+nest_status nest_batch_totals(nest_batch* b, double* out) {
+    nest_status r = batch_check(b);
+    if (r != NEST_OK) return r;
+    if (!b->partials) return fail(NEST_ERR_UNSUPPORTED, "totals need a batch created with NEST_FLAG_TOTALS");
+    cudaError_t e = launch_sum_batch(b->partials, b->dfirst, b->count, b->totals_dev, b->st);
+    if (e != cudaSuccess) return cuda_fail(e, "batch totals kernel");
+    CK(cudaMemcpyAsync(out, b->totals_dev, sizeof(double) * 4 * b->count, cudaMemcpyDeviceToHost, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    for (int p = 0; p < b->count; ++p)
+        for (int k = 0; k < 4; ++k) out[4 * p + k] *= b->probs[p].g.dx * b->probs[p].g.dy;
+    return NEST_OK;
+}
+
+nest_status nest_batch_info(nest_batch* b, long long* cells, int* items, int* blocks) {
+    nest_status r = batch_check(b);
+    if (r != NEST_OK) return r;
+    long long c = 0;
+    for (auto& p : b->probs) c += (long long)p.g.nx * p.g.ny;
+    if (cells) *cells = c;
+    if (items) *items = (int)b->items.size();
+    if (blocks) *blocks = b->blocks;
+    return NEST_OK;
 }
 
 }  // extern "C"

@@ -103,12 +103,12 @@ __device__ __forceinline__ F2 yslope(F2 w) {
     return make_float2(mm(e.x, e.y), mm(e.y, ra - w.y));
 }
 
+// One warp's work: the rows of tile `tile_row` under column strip `strip`.
+// The warp owning strip 0 / tile 0 publishes the step's dt for the domain.
 template <int STAGE, bool REPAIR>
-__global__ void __launch_bounds__(256) k2d_f32x2(StageArgs<float> a) {
+__device__ __forceinline__ void x2_body(const StageArgs<float>& a, int strip, int tile_row) {
     const Geo2D& g = a.g;
     const int lane = threadIdx.x & 31;
-    const int strip = blockIdx.x * blockDim.y + threadIdx.y;
-    const int tile_row = blockIdx.y;
     const float gamma = (float)g.gamma;
     const float gm1 = (float)(g.gamma - 1.0);
     const float igm1 = (float)(1.0 / (g.gamma - 1.0));
@@ -124,8 +124,7 @@ __global__ void __launch_bounds__(256) k2d_f32x2(StageArgs<float> a) {
                                 g.dx, g.dy, a.lp.cfl);
             if (a.lp.t_final > 0.0) dt = smin(dt, a.lp.t_final - a.ctrl->time[a.p]);
         }
-        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0)
-            publish_step(a.ctrl, a.p, a.lp, done, dt);
+        if (strip == 0 && tile_row == 0 && lane == 0) publish_step(a.ctrl, a.p, a.lp, done, dt);
         if (done) return;
     } else {
         if (!a.ctrl->active[a.p]) return;
@@ -301,7 +300,7 @@ __global__ void __launch_bounds__(256) k2d_f32x2(StageArgs<float> a) {
         if (a.partials) {
             t0 = warp_sum(t0); t1 = warp_sum(t1); t2 = warp_sum(t2); t3 = warp_sum(t3);
             if (lane == 0) {
-                long long wid = ((long long)tile_row * ((g.ny + STRIP2 - 1) / STRIP2) + strip) * 4;
+                long long wid = ((long long)tile_row * ((g.ny + STRIP2 - 1) / STRIP2) + strip) * 4;  // per-domain slot
                 a.partials[wid + 0] = t0; a.partials[wid + 1] = t1;
                 a.partials[wid + 2] = t2; a.partials[wid + 3] = t3;
             }
@@ -309,9 +308,49 @@ __global__ void __launch_bounds__(256) k2d_f32x2(StageArgs<float> a) {
     }
 }
 
+template <int STAGE, bool REPAIR>
+__global__ void __launch_bounds__(256) k2d_f32x2(StageArgs<float> a) {
+    x2_body<STAGE, REPAIR>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+}
+
+// Persistent batched stage: every warp walks the work list (problem, strip,
+// tile row) with a stride of the whole grid's warp count.
+template <int STAGE, bool REPAIR>
+__global__ void __launch_bounds__(256) kbatch_f32x2(BatchArgs<float> b) {
+    const int nw = gridDim.x * blockDim.y;
+    for (int it = blockIdx.x * blockDim.y + threadIdx.y; it < b.nitems; it += nw) {
+        const int4 w = b.items[it];
+        const BatchProblem& P = b.probs[w.x];
+        StageArgs<float> a{STAGE == 1 ? b.U + P.off : b.U1 + P.off, STAGE == 2 ? b.U + P.off : nullptr,
+                           STAGE == 1 ? b.U1 + P.off : b.U + P.off, P.g, b.lp, b.ctrls + w.x,
+                           (STAGE == 2 && b.partials) ? b.partials + 4ll * P.item0 : nullptr, b.p, b.tx};
+        x2_body<STAGE, REPAIR>(a, w.y, w.z);
+    }
+}
+
 }  // namespace
 
 int strips_f32x2(int ny) { return (ny + STRIP2 - 1) / STRIP2; }
+
+cudaError_t launch_batch_f32x2(const BatchArgs<float>& b, bool repair, int which, int blocks, int warps,
+                               cudaStream_t st) {
+    dim3 blk(32, warps);
+    BatchArgs<float> b1 = b, b2 = b;
+    if (repair) {
+        if (which & 1) kbatch_f32x2<1, true><<<blocks, blk, 0, st>>>(b1);
+        if (which & 2) kbatch_f32x2<2, true><<<blocks, blk, 0, st>>>(b2);
+    } else {
+        if (which & 1) kbatch_f32x2<1, false><<<blocks, blk, 0, st>>>(b1);
+        if (which & 2) kbatch_f32x2<2, false><<<blocks, blk, 0, st>>>(b2);
+    }
+    return cudaGetLastError();
+}
+
+int batch_max_blocks_f32x2(int warps) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kbatch_f32x2<2, false>, 32 * warps, 0);
+    return nb;
+}
 
 cudaError_t launch_2d_step_f32x2(float* U, float* U1, const Geo2D& g, const LoopParams& lp, StepCtrl* ctrl,
                                  double* partials, int p, int tx, int warps, bool repair, int which,

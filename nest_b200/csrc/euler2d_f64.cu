@@ -33,6 +33,57 @@ cudaError_t launch_2d_step_f64(double* U, double* U1, const Geo2D& g, const Loop
     return cudaGetLastError();
 }
 
+// Persistent batched FP64 stage (bit-exact per problem).
+template <int STAGE>
+__global__ void __launch_bounds__(256) kbatch_f64(BatchArgs<double> b) {
+    const int nw = gridDim.x * blockDim.y;
+    for (int it = blockIdx.x * blockDim.y + threadIdx.y; it < b.nitems; it += nw) {
+        const int4 w = b.items[it];
+        const BatchProblem& P = b.probs[w.x];
+        StageArgs<double> a{STAGE == 1 ? b.U + P.off : b.U1 + P.off, STAGE == 2 ? b.U + P.off : nullptr,
+                            STAGE == 1 ? b.U1 + P.off : b.U + P.off, P.g, b.lp, b.ctrls + w.x,
+                            (STAGE == 2 && b.partials) ? b.partials + 4ll * P.item0 : nullptr, b.p, b.tx};
+        stage2d_body<double, STAGE, false>(a, w.y, w.z);
+    }
+}
+
+cudaError_t launch_batch_f64(const BatchArgs<double>& b, int which, int blocks, int warps, cudaStream_t st) {
+    dim3 blk(32, warps);
+    if (which & 1) kbatch_f64<1><<<blocks, blk, 0, st>>>(b);
+    if (which & 2) kbatch_f64<2><<<blocks, blk, 0, st>>>(b);
+    return cudaGetLastError();
+}
+
+int batch_max_blocks_f64(int warps) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kbatch_f64<2>, 32 * warps, 0);
+    return nb;
+}
+
+// Per-problem deterministic sums of the per-item totals: block p sums items
+// [first[p], first[p+1]) in a fixed order.
+__global__ void __launch_bounds__(256) k_sum_batch(const double* part, const int* first, double* out) {
+    __shared__ double s[4][256];
+    int p = blockIdx.x;
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (long long r = first[p] + threadIdx.x; r < first[p + 1]; r += 256) {
+        a0 += part[4 * r]; a1 += part[4 * r + 1]; a2 += part[4 * r + 2]; a3 += part[4 * r + 3];
+    }
+    s[0][threadIdx.x] = a0; s[1][threadIdx.x] = a1; s[2][threadIdx.x] = a2; s[3][threadIdx.x] = a3;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int k = 0; k < 4; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) out[4 * p + threadIdx.x] = s[threadIdx.x][0];
+}
+
+cudaError_t launch_sum_batch(const double* partials, const int* first, int count, double* out, cudaStream_t st) {
+    k_sum_batch<<<count, 256, 0, st>>>(partials, first, out);
+    return cudaGetLastError();
+}
+
 // Deterministic sum of per-warp totals: one block, fixed strided order, fixed tree.
 __global__ void __launch_bounds__(256) k_sum_partials(const double* part, long long nrec, double* out) {
     __shared__ double s[4][256];

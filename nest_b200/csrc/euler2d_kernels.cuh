@@ -247,8 +247,7 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
                                 g.dx, g.dy, a.lp.cfl);
             if (a.lp.t_final > 0.0) dt = smin(dt, a.lp.t_final - a.ctrl->time[a.p]);
         }
-        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0)
-            publish_step(a.ctrl, a.p, a.lp, done, dt);
+        if (strip == 0 && tile_row == 0 && lane == 0) publish_step(a.ctrl, a.p, a.lp, done, dt);
         if (done) return;
     } else {
         if (!a.ctrl->active[a.p]) return;
@@ -386,6 +385,30 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
         }
     }
 }
+
+// One problem of a batch: its geometry, the offset of its arrays inside the
+// batch buffers, and the index of its first work item (its totals slots).
+struct BatchProblem {
+    Geo2D g;
+    long long off;
+    int item0;
+    int pad;
+};
+
+// Arguments of a persistent batched stage launch.
+template <typename T>
+struct BatchArgs {
+    T* U;                       // all problems' states, problem p at U + probs[p].off
+    T* U1;                      // stage buffers, same offsets
+    const BatchProblem* probs;
+    const int4* items;          // (problem, strip, tile row, 0)
+    int nitems;
+    StepCtrl* ctrls;            // one control block per problem
+    double* partials;           // per-item FP64 totals (stage 2) or null
+    LoopParams lp;
+    int p;
+    int tx;
+};
 
 // Ghost ring (faces and corners) and wave-speed maxima of the current state
 // into slot p.  Run once after an upload or an external state change.

@@ -39,6 +39,16 @@ cudaError_t launch_2d_step_f32x2(float* U, float* U1, const Geo2D& g, const Loop
                                  double* partials, int p, int tx, int warps, bool repair, int which,
                                  cudaStream_t st);
 
+// Batched persistent stages (one launch per stage over the work list).
+template <typename T> struct BatchArgs;
+cudaError_t launch_batch_f64(const BatchArgs<double>& b, int which, int blocks, int warps, cudaStream_t st);
+cudaError_t launch_batch_f32x2(const BatchArgs<float>& b, bool repair, int which, int blocks, int warps,
+                               cudaStream_t st);
+int batch_max_blocks_f64(int warps);
+int batch_max_blocks_f32x2(int warps);
+int strips_f32x2(int ny);
+cudaError_t launch_sum_batch(const double* partials, const int* first, int count, double* out, cudaStream_t st);
+
 // Records msg as the calling thread's last error (read by nest_last_error()).
 nest_status record_error(nest_status st, const std::string& msg);
 
