@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--tiling", default="", help="rows,warps: fixed launch shape instead of the tuned one")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched-KH and adjoint measurements")
+    ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--batch-steps", type=int, default=500)
+    ap.add_argument("--adjoint-n", type=int, default=65536)
+    ap.add_argument("--adjoint-steps", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -284,9 +289,87 @@ def run_ours(args, ws, rank, local):
         "clocks": clk,
         "gpu_launches": launches,
     }
+    if not args.no_extras:
+        out["batched_kh"] = bench_batch(args, ws)
+        out["adjoint_1d"] = bench_adjoint(args)
+        out["gpu_launches_extras"] = out["batched_kh"]["launches"] + out["adjoint_1d"]["launches"]
     if ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(n, args.cpu_seconds)
     return out
+
+
+def bench_batch(args, ws):
+    """Batched Kelvin-Helmholtz: `count` independent periodic problems with
+    sides drawn uniformly from {64, ..., 1024} (seed 0), FP32 state with FP64
+    totals and repair, one persistent launch per stage, steps replayed from
+    captured CUDA graphs; K = batch_steps steps per problem."""
+    import torch
+    import nest_b200 as nb
+    from nest_b200.problems import kelvin_helmholtz, kh_sizes
+    nx, ny = kh_sizes(args.batch_count, seed=0)
+    st = torch.cuda.Stream()
+    from nest_b200.tuning import best_batch_tiling
+    b = nb.Batch(nx, ny, precision=nb.F32, flags=nb.FLAG_TOTALS | nb.FLAG_REPAIR, stream=st.cuda_stream)
+    ics = [kelvin_helmholtz(int(nx[p]), int(ny[p]), seed=1 + p).astype(np.float32) for p in range(len(nx))]
+    for p, U in enumerate(ics):
+        b.upload(p, U)
+    tiling = best_batch_tiling(b, nx, ny)  # may advance the states: re-upload below
+    b.set_tiling(*tiling)
+    for p, U in enumerate(ics):
+        b.upload(p, U)
+    b.reset()
+    del ics
+    cells, items, blocks = b.info()
+    b.step(2, 0.4)
+    torch.cuda.synchronize()
+    t0 = b.totals().copy()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    b.step(args.batch_steps, 0.4)
+    e1.record(st)
+    e1.synchronize()
+    ms = allmax(ws, e0.elapsed_time(e1))
+    times, steps = b.times()
+    tot = b.totals()
+    drift = np.abs(tot - t0).max(axis=0) / np.maximum(np.abs(t0).max(axis=0), 1e-300)
+    value = ws * cells * 2 * args.batch_steps / (ms * 1e-3)
+    b.close()
+    return {"value": value, "unit": UNIT, "problems": int(len(nx)), "cells": int(cells), "steps": args.batch_steps,
+            "ms_total": ms, "ms_per_step": ms / args.batch_steps, "work_items": items, "persistent_blocks": blocks,
+            "hbm_gbs_equiv": value / ws * 40 / 1e9, "sim_time_range": [float(times.min()), float(times.max())],
+            "fp64_totals_rel_drift": {"mass": float(drift[0]), "energy": float(drift[3])},
+            "tiling": {"rows_per_item": tiling[0], "warps_per_block": tiling[1], "blocks_per_sm": tiling[2]},
+            "launches": 2 * args.batch_steps, "dtype": "f32 (FP64 totals, time, repair)"}
+
+
+def bench_adjoint(args):
+    """1D adjoint workload: N periodic cells, Fourier initial state (seeds 1
+    and 2), K steps at CFL 0.4, loss 1/2 sum (rho_T - rho_target)^2 dx,
+    checkpoint every 64 steps; forward sweep (CFL, dts recorded) and
+    backward sweep (segment recompute + adjoint) timed separately."""
+    import nest_b200 as nb
+    from nest_b200.adjoint import Adjoint
+    from nest_b200.problems import fourier_fields_1d, prim_to_cons_1d
+    n, K = args.adjoint_n, args.adjoint_steps
+    U0 = prim_to_cons_1d(*fourier_fields_1d(n, seed=1))
+    tgt = prim_to_cons_1d(*fourier_fields_1d(n, seed=2))[0, 2:-2]
+    s = nb.Solver(1, n, bc=nb.BC_PERIODIC, flags=nb.FLAG_NO_RESIDENT)
+    s.upload(U0)
+    a = Adjoint(s, K, 0, 64)
+    a.forward(0.4)  # warm (graph capture, first launches)
+    s.upload(U0)
+    a = Adjoint(s, K, 0, 64)
+    a.forward(0.4)
+    UT = s.download()
+    lam = np.zeros_like(UT)
+    lam[0, 2:-2] = (UT[0, 2:-2] - tgt) / n
+    a.backward(lam)
+    st = a.stats()
+    fwd, bwd = st["forward_ms"], st["backward_ms"]
+    return {"n": n, "steps": K, "checkpoint_every": 64, "forward_ms": fwd, "backward_ms": bwd,
+            "adjoint_over_forward": bwd / fwd, "gradient_over_forward": (fwd + bwd) / fwd,
+            "recomputed_steps": st["recomputed_steps"], "checkpoint_mb": st["checkpoint_bytes"] / 1e6,
+            "launches": 2 * K + 2 * K + 3 * K, "dtype": "f64"}
 
 
 def e2e_run(s, U, steps, cfl, st, cells, ws):

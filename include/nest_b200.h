@@ -50,7 +50,9 @@ enum {
     NEST_FLAG_TOTALS = 1,       /* keep FP64 conserved totals each step (2D) */
     NEST_FLAG_REPAIR = 2,       /* FP32 form: FP64 positivity repair near vacuum */
     NEST_FLAG_NO_RESIDENT = 4,  /* 1D: never use the single-CTA resident solver */
-    NEST_FLAG_FP32_SCALAR = 8   /* FP32 form: one column per lane instead of packed FP32x2 pairs */
+    NEST_FLAG_FP32_SCALAR = 8,  /* FP32 form: one column per lane instead of packed FP32x2 pairs */
+    NEST_FLAG_SPLIT_COMPAT = 16 /* 2D FP64: nest's own dimensionally split forward-Euler sweeps
+                                   (examples/sod2d/euler2d.hpp:67-271) instead of unsplit RK2 */
 };
 
 /* ------------------------------------------------------------------------ */
@@ -182,8 +184,56 @@ nest_status nest_batch_times(nest_batch* b, double* times, int* steps);
 nest_status nest_batch_totals(nest_batch* b, double* out);
 /* Launch shape: rows per work item, warps per block, blocks per SM (0 = occupancy limit). */
 nest_status nest_batch_set_tiling(nest_batch* b, int rows_per_tile, int warps_per_block, int blocks_per_sm);
+/* Zero every problem's time, step count and error word (states are kept;
+ * ghost rings and wave speeds are rebuilt before the next step). */
+nest_status nest_batch_reset(nest_batch* b);
 /* Total interior cells, work items and persistent blocks. */
 nest_status nest_batch_info(nest_batch* b, long long* cells, int* items, int* blocks);
+
+/* ------------------------------------------------------------------------ */
+/* Patch halo exchange on nest's per-patch storage (device).                */
+/* Plan = build_periodic_mesh_1d / _2d (include/nest/patch.hpp:88-147,      */
+/* 207-326); execute = execute_all_exchanges (patch.hpp:153-190) in one     */
+/* kernel launch.  Patches are stored one after another in patch order,     */
+/* each as nvars SoA planes over its extended space, idx[1] fastest.        */
+/* ------------------------------------------------------------------------ */
+typedef struct nest_exchange nest_exchange;
+/* dim 1: nx cells in npx patches (ny, npy ignored); dim 2: nx x ny in npx x npy. */
+nest_status nest_exchange_create_periodic(int dim, int nx, int ny, int npx, int npy, int nvars, int halo,
+                                          nest_exchange** out);
+nest_status nest_exchange_destroy(nest_exchange* x);
+/* Element offset of each patch block (npatches + 1 values), interior boxes
+ * (start0, start1, shape0, shape1 per patch) and the peer of every region
+ * (2 per patch in 1D, 4 in 2D, in nest's order); any pointer may be NULL. */
+nest_status nest_exchange_layout(nest_exchange* x, long long* offsets, int* boxes, int* peers);
+/* Fill every patch's face halos from its periodic neighbours (device data). */
+nest_status nest_exchange_execute(nest_exchange* x, void* d_data, int precision, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Discrete adjoint with checkpointing.  No counterpart in nest.            */
+/* The forward sweep runs the solver from its current state for nsteps with */
+/* CFL dt (recorded) or a given dt sequence; the backward sweep maps the    */
+/* adjoint of the final state to the adjoint of the initial state with the  */
+/* same frozen dts.  Memory is bounded by checkpoint-and-recompute:         */
+/*   NEST_CKPT_UNIFORM  param = K: a checkpoint every K steps;              */
+/*   NEST_CKPT_BINOMIAL param = s: s snapshot slots, binomial schedule.     */
+/* Adjoint arrays use the solver's device layout (1D: [3][n + 2h]); on      */
+/* device or host memory.  This build: 1D FP64, periodic.                   */
+/* ------------------------------------------------------------------------ */
+enum { NEST_CKPT_UNIFORM = 0, NEST_CKPT_BINOMIAL = 1 };
+typedef struct nest_adjoint nest_adjoint;
+/* The adjoint object refers to its solver: destroy it before the solver, or
+ * after (destroy never touches the solver). */
+nest_status nest_adjoint_create(nest_solver* s, int nsteps, int policy, int param, nest_adjoint** out);
+nest_status nest_adjoint_destroy(nest_adjoint* a);
+/* dts: NULL for CFL dt (recorded), else nsteps frozen values. */
+nest_status nest_adjoint_forward(nest_adjoint* a, double cfl, const double* dts);
+nest_status nest_adjoint_backward(nest_adjoint* a, const void* lam_final, void* lam_initial, int on_device);
+nest_status nest_adjoint_get_dts(nest_adjoint* a, double* dts);
+/* Wall-clock ms of the two sweeps, forward steps recomputed by the backward
+ * sweep, and device bytes held for checkpoints and work buffers. */
+nest_status nest_adjoint_stats(nest_adjoint* a, double* fwd_ms, double* bwd_ms, long long* recomputed_steps,
+                               long long* snapshot_bytes);
 
 /* ------------------------------------------------------------------------ */
 /* Allocation-free 1D run.  No counterpart in nest's ABI.                   */

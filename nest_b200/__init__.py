@@ -5,12 +5,14 @@ include/nest_b200.h).  Importing this package loads it; there is no CPU
 fallback.
 """
 from ._capi import (BC_OUTFLOW, BC_PERIODIC, F32, F64, FLAG_FP32_SCALAR, FLAG_NO_RESIDENT, FLAG_REPAIR,
+                    FLAG_SPLIT_COMPAT,
                     FLAG_TOTALS, LAYOUT_EXTENDED, LAYOUT_INTERIOR, LIB_PATH, NestError)
 from .batch import Batch
+from .exchange import PeriodicExchange
 from .solver import Euler1DGPU, Solver
 
 __all__ = [
-    "Batch", "Euler1DGPU", "Solver", "NestError", "BC_PERIODIC", "BC_OUTFLOW", "F64", "F32",
-    "LAYOUT_EXTENDED", "LAYOUT_INTERIOR", "FLAG_TOTALS", "FLAG_REPAIR", "FLAG_NO_RESIDENT", "FLAG_FP32_SCALAR",
+    "Batch", "PeriodicExchange", "Euler1DGPU", "Solver", "NestError", "BC_PERIODIC", "BC_OUTFLOW", "F64", "F32",
+    "LAYOUT_EXTENDED", "LAYOUT_INTERIOR", "FLAG_TOTALS", "FLAG_REPAIR", "FLAG_NO_RESIDENT", "FLAG_FP32_SCALAR", "FLAG_SPLIT_COMPAT",
     "LIB_PATH",
 ]

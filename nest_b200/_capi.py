@@ -21,7 +21,7 @@ STATUS_NAMES = {
 BC_PERIODIC, BC_OUTFLOW = 0, 1
 F64, F32 = 0, 1
 LAYOUT_EXTENDED, LAYOUT_INTERIOR = 0, 1
-FLAG_TOTALS, FLAG_REPAIR, FLAG_NO_RESIDENT, FLAG_FP32_SCALAR = 1, 2, 4, 8
+FLAG_TOTALS, FLAG_REPAIR, FLAG_NO_RESIDENT, FLAG_FP32_SCALAR, FLAG_SPLIT_COMPAT = 1, 2, 4, 8, 16
 
 
 class NestError(RuntimeError):

@@ -29,6 +29,7 @@ A.bind({
     "nest_batch_totals": (_i, [_vp, C.POINTER(C.c_double)]),
     "nest_batch_set_tiling": (_i, [_vp, _i, _i, _i]),
     "nest_batch_info": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "nest_batch_reset": (_i, [_vp]),
 })
 
 
@@ -94,6 +95,9 @@ class Batch:
     def set_tiling(self, rows_per_tile: int, warps_per_block: int, blocks_per_sm: int = 0):
         check(lib.nest_batch_set_tiling(self._h, rows_per_tile, warps_per_block, blocks_per_sm),
               "nest_batch_set_tiling")
+
+    def reset(self):
+        check(lib.nest_batch_reset(self._h), "nest_batch_reset")
 
     def info(self):
         c, it, bl = C.c_longlong(), C.c_int(), C.c_int()

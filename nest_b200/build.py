@@ -29,8 +29,12 @@ UNITS = {
     "euler2d_f64.cu": ["-fmad=false"],
     "euler2d_f32.cu": ["-use_fast_math"],
     "euler2d_f32x2.cu": ["-use_fast_math"],
+    "euler2d_compat.cu": ["-fmad=false"],
     "capi.cpp": ["-x", "cu"],
     "noalloc.cu": [],
+    "adjoint1d.cu": [],
+    "adjoint.cpp": ["-x", "cu"],
+    "exchange.cu": [],
 }
 
 

@@ -1,0 +1,349 @@
+// Checkpointed discrete adjoint of a solver's time loop (C++ host runtime).
+//
+// The forward sweep runs the solver's own step path with CFL dt and records
+// the dt sequence; the adjoint then uses that frozen sequence.  Memory is
+// bounded by checkpoint-and-recompute:
+//   NEST_CKPT_UNIFORM  (param K): the forward sweep stores U every K steps;
+//      each segment is recomputed once, storing its K states (and the stage
+//      states U1), then reversed.  Cost: two forward sweeps.
+//   NEST_CKPT_BINOMIAL (param s): s snapshot slots, schedule by the binomial
+//      recursion of Griewank & Walther ("revolve", ACM TOMS 26(1), 2000):
+//      with beta(s, r) = C(s + r, s), a range of t <= beta(s, r) steps is
+//      split at d = beta(s, r - 1) from its start; the right part is reversed
+//      first with s - 1 free slots, then the left part with s.  A slot cache
+//      lets the recursion reuse the snapshots the forward sweep took along
+//      the rightmost spine.
+// Per reversed step: one stage-1 recompute of U1 from U^n, then
+//   tmp      = 1/2 * S'(U1)^T lambda^{n+1}
+//   lambda^n = S'(U^n)^T tmp + 1/2 lambda^{n+1}
+// (Heun: U^{n+1} = 1/2 (U^n + S(S(U^n)))).
+#include <algorithm>
+#include <chrono>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "solver_impl.h"
+
+using namespace nestb;
+using namespace nestb::rt;
+
+namespace nestb {
+cudaError_t launch_1d_adjoint_stage(const double* U, const double* Lout, const double* Extra, double* Lin, int n,
+                                    int h, double lambda, double gamma, double alpha, double beta,
+                                    cudaStream_t st);
+}
+
+namespace {
+
+// Device operations the schedules need, for one solver form.
+struct Stepper {
+    virtual ~Stepper() = default;
+    virtual cudaError_t step(void* U, void* U1, double dt) = 0;          // U <- Heun step (U1 scratch)
+    virtual cudaError_t stage1(void* U, void* U1, double dt) = 0;        // U1 <- S(U)
+    virtual cudaError_t stage2(void* U, void* U1, double dt) = 0;        // U <- (U + S(U1)) / 2 after stage1
+    virtual cudaError_t adjoint_step(void* Un, void* U1, double dt, void* lam, void* lam_new, void* tmp) = 0;
+};
+
+struct Stepper1D : Stepper {
+    nest_solver* s;
+    StepCtrl* ctrl;
+    explicit Stepper1D(nest_solver* s_, StepCtrl* c) : s(s_), ctrl(c) {}
+    LoopParams lp(double dt) const {
+        LoopParams p{};
+        p.cfl = 1.0;
+        p.fixed_dt = dt;
+        return p;
+    }
+    cudaError_t step(void* U, void* U1, double dt) override {
+        return launch_1d_step((double*)U, (double*)U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp(dt),
+                              ctrl, 0, 3, s->st);
+    }
+    cudaError_t stage1(void* U, void* U1, double dt) override {
+        return launch_1d_step((double*)U, (double*)U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp(dt),
+                              ctrl, 0, 1, s->st);
+    }
+    cudaError_t stage2(void* U, void* U1, double dt) override {
+        return launch_1d_step((double*)U, (double*)U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp(dt),
+                              ctrl, 0, 2, s->st);
+    }
+    cudaError_t adjoint_step(void* Un, void* U1, double dt, void* lam, void* lam_new, void* tmp) override {
+        double l = dt / s->d.dx;
+        cudaError_t e = launch_1d_adjoint_stage((const double*)U1, (const double*)lam, nullptr, (double*)tmp,
+                                                s->d.nx, s->h, l, s->d.gamma, 0.5, 0.0, s->st);
+        if (e != cudaSuccess) return e;
+        return launch_1d_adjoint_stage((const double*)Un, (const double*)tmp, (const double*)lam,
+                                       (double*)lam_new, s->d.nx, s->h, l, s->d.gamma, 1.0, 0.5, s->st);
+    }
+};
+
+long long binom(int n, int k) {  // C(n, k), saturating
+    if (k < 0 || k > n) return 0;
+    long double r = 1;
+    for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+    return r > 9.0e18L ? (long long)9.0e18 : (long long)(r + 0.5L);
+}
+
+}  // namespace
+
+struct nest_adjoint {
+    nest_solver* s = nullptr;
+    int nsteps = 0, policy = 0, param = 0;
+    std::unique_ptr<Stepper> stepper;
+    StepCtrl* ctrl = nullptr;
+    std::vector<double> dts;
+    std::vector<void*> slots;      // snapshot slots (binomial) or checkpoints (uniform)
+    std::vector<int> slot_pos;     // step index held by each slot (-1: none)
+    std::vector<void*> seg_un, seg_u1;  // uniform: states of one segment
+    void* work = nullptr;
+    void* u1 = nullptr;
+    void* lam[2] = {nullptr, nullptr};
+    void* tmp = nullptr;
+    bool forward_done = false;
+    double fwd_ms = 0.0, bwd_ms = 0.0;
+    long long advanced = 0;        // forward steps run by the backward sweep (recompute)
+    long long snap_bytes = 0;
+};
+
+namespace {
+
+nest_status adj_alloc(nest_adjoint* a, void** p) {
+    CK(cudaMalloc(p, a->s->state_bytes()));
+    CK(cudaMemsetAsync(*p, 0, a->s->state_bytes(), a->s->st));
+    a->snap_bytes += (long long)a->s->state_bytes();
+    return NEST_OK;
+}
+
+nest_status copy_state_dev(nest_adjoint* a, void* dst, const void* src) {
+    CK(cudaMemcpyAsync(dst, src, a->s->state_bytes(), cudaMemcpyDeviceToDevice, a->s->st));
+    return NEST_OK;
+}
+
+// Advance `work` (holding the state at step j0) by k steps.
+nest_status advance_work(nest_adjoint* a, int j0, int k) {
+    for (int j = j0; j < j0 + k; ++j) {
+        cudaError_t e = a->stepper->step(a->work, a->u1, a->dts[j]);
+        if (e != cudaSuccess) return cuda_fail(e, "recompute step");
+        ++a->advanced;
+    }
+    return NEST_OK;
+}
+
+// lambda <- adjoint of step j applied to lambda, given U^n of step j in `un`.
+nest_status reverse_one(nest_adjoint* a, void* un, int j, int& cur) {
+    cudaError_t e = a->stepper->stage1(un, a->u1, a->dts[j]);
+    if (e == cudaSuccess) e = a->stepper->adjoint_step(un, a->u1, a->dts[j], a->lam[cur], a->lam[cur ^ 1], a->tmp);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint step");
+    cur ^= 1;
+    return NEST_OK;
+}
+
+// Binomial reversal of steps [l, r); the state at l is in slot k; slots
+// k+1 .. k+free are available.
+nest_status reverse_binomial(nest_adjoint* a, int l, int r, int k, int free, int& cur) {
+    nest_status st;
+    int t = r - l;
+    if (t == 1) return reverse_one(a, a->slots[k], l, cur);
+    if (free == 0) {
+        for (int j = r - 1; j >= l; --j) {
+            if ((st = copy_state_dev(a, a->work, a->slots[k])) != NEST_OK) return st;
+            if ((st = advance_work(a, l, j - l)) != NEST_OK) return st;
+            if ((st = reverse_one(a, a->work, j, cur)) != NEST_OK) return st;
+        }
+        return NEST_OK;
+    }
+    int rep = 1;
+    while (binom(free + rep, free) < t) ++rep;
+    long long d = binom(free + rep - 1, free);  // beta(free, rep - 1)
+    d = std::max<long long>(1, std::min<long long>(d, t - 1));
+    int m = l + (int)d;
+    if (a->slot_pos[k + 1] != m) {
+        if ((st = copy_state_dev(a, a->work, a->slots[k])) != NEST_OK) return st;
+        if ((st = advance_work(a, l, m - l)) != NEST_OK) return st;
+        if ((st = copy_state_dev(a, a->slots[k + 1], a->work)) != NEST_OK) return st;
+        a->slot_pos[k + 1] = m;
+    }
+    if ((st = reverse_binomial(a, m, r, k + 1, free - 1, cur)) != NEST_OK) return st;
+    a->slot_pos[k + 1] = -1;
+    return reverse_binomial(a, l, m, k, free, cur);
+}
+
+// Steps at which the forward sweep stores snapshots: uniform multiples of K,
+// or the rightmost spine of the binomial recursion.
+std::vector<std::pair<int, int>> forward_snapshots(const nest_adjoint* a) {
+    std::vector<std::pair<int, int>> v;  // (step, slot)
+    if (a->policy == NEST_CKPT_UNIFORM) {
+        for (int j = 0, k = 0; j < a->nsteps; j += a->param, ++k) v.push_back({j, k});
+        return v;
+    }
+    int l = 0, r = a->nsteps, k = 0, free = a->param - 1;
+    v.push_back({0, 0});
+    while (r - l > 1 && free > 0) {
+        int t = r - l, rep = 1;
+        while (binom(free + rep, free) < t) ++rep;
+        long long d = std::max<long long>(1, std::min<long long>(binom(free + rep - 1, free), t - 1));
+        l += (int)d;
+        ++k;
+        --free;
+        v.push_back({l, k});
+    }
+    return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+nest_status nest_adjoint_create(nest_solver* s, int nsteps, int policy, int param, nest_adjoint** out) {
+    if (!s || !out) return fail(NEST_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (nsteps <= 0) return fail(NEST_ERR_INVALID, "nsteps must be positive");
+    if (policy != NEST_CKPT_UNIFORM && policy != NEST_CKPT_BINOMIAL) return fail(NEST_ERR_INVALID, "bad policy");
+    if (param < 1) return fail(NEST_ERR_INVALID, "checkpoint parameter must be >= 1");
+    if (s->d.dim != 1 || s->d.precision != NEST_F64)
+        return fail(NEST_ERR_UNSUPPORTED, "adjoint: this build supports the 1D FP64 solver");
+    if (s->d.bc_x != NEST_BC_PERIODIC) return fail(NEST_ERR_UNSUPPORTED, "adjoint: periodic boundaries");
+    auto* a = new (std::nothrow) nest_adjoint;
+    if (!a) return fail(NEST_ERR_OOM, "host allocation failed");
+    a->s = s;
+    a->nsteps = nsteps;
+    a->policy = policy;
+    a->param = policy == NEST_CKPT_UNIFORM ? std::min(param, nsteps) : std::min(param, nsteps);
+    auto cleanup = [&](nest_status st) { nest_adjoint_destroy(a); return st; };
+    cudaError_t e = cudaMalloc(&a->ctrl, sizeof(StepCtrl));
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(ctrl)"));
+    if ((e = cudaMemset(a->ctrl, 0, sizeof(StepCtrl))) != cudaSuccess) return cleanup(cuda_fail(e, "memset"));
+    a->stepper.reset(new Stepper1D(s, a->ctrl));
+    nest_status st;
+    int nslots = policy == NEST_CKPT_UNIFORM ? (nsteps + a->param - 1) / a->param : a->param;
+    a->slots.assign(nslots, nullptr);
+    a->slot_pos.assign(nslots + 1, -1);
+    for (auto& p : a->slots)
+        if ((st = adj_alloc(a, &p)) != NEST_OK) return cleanup(st);
+    if (policy == NEST_CKPT_UNIFORM) {
+        a->seg_un.assign(a->param, nullptr);
+        a->seg_u1.assign(a->param, nullptr);
+        for (int i = 0; i < a->param; ++i) {
+            if ((st = adj_alloc(a, &a->seg_un[i])) != NEST_OK) return cleanup(st);
+            if ((st = adj_alloc(a, &a->seg_u1[i])) != NEST_OK) return cleanup(st);
+        }
+    }
+    for (void** p : {&a->work, &a->u1, &a->lam[0], &a->lam[1], &a->tmp})
+        if ((st = adj_alloc(a, p)) != NEST_OK) return cleanup(st);
+    *out = a;
+    return NEST_OK;
+}
+
+nest_status nest_adjoint_destroy(nest_adjoint* a) {
+    // Does not touch the solver (it may already be destroyed); cudaFree waits
+    // for outstanding work on these buffers.
+    if (!a) return NEST_OK;
+    for (void* p : a->slots) cudaFree(p);
+    for (void* p : a->seg_un) cudaFree(p);
+    for (void* p : a->seg_u1) cudaFree(p);
+    for (void* p : {a->work, a->u1, a->lam[0], a->lam[1], a->tmp}) cudaFree(p);
+    cudaFree(a->ctrl);
+    delete a;
+    return NEST_OK;
+}
+
+nest_status nest_adjoint_forward(nest_adjoint* a, double cfl, const double* dts) {
+    if (!a) return fail(NEST_ERR_INVALID, "null adjoint handle");
+    nest_solver* s = a->s;
+    nest_status st;
+    if ((st = nest_solver_reset_time(s)) != NEST_OK) return st;
+    if (dts) {
+        a->dts.assign(dts, dts + a->nsteps);
+        if ((st = nest_solver_set_dt_sequence(s, dts, a->nsteps, 0)) != NEST_OK) return st;
+    } else {
+        if ((st = nest_solver_set_dt_sequence(s, nullptr, a->nsteps, 1)) != NEST_OK) return st;
+    }
+    if (!s->prepared && (st = prepare(s)) != NEST_OK) return st;
+    auto snaps = forward_snapshots(a);
+    std::fill(a->slot_pos.begin(), a->slot_pos.end(), -1);
+    CK(cudaStreamSynchronize(s->st));
+    auto t0 = std::chrono::high_resolution_clock::now();
+    int at = 0;
+    for (auto [step, slot] : snaps) {
+        if (step > at) {
+            if ((st = nest_solver_step(s, step - at, cfl)) != NEST_OK) return st;
+            at = step;
+        }
+        if ((st = copy_state_dev(a, a->slots[slot], s->U)) != NEST_OK) return st;
+        a->slot_pos[slot] = step;
+    }
+    if (a->nsteps > at && (st = nest_solver_step(s, a->nsteps - at, cfl)) != NEST_OK) return st;
+    if ((st = read_ctrl(s)) != NEST_OK) return st;
+    auto t1 = std::chrono::high_resolution_clock::now();
+    a->fwd_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    if (!dts) {
+        a->dts.resize(a->nsteps);
+        if ((st = nest_solver_get_dts(s, a->dts.data(), a->nsteps)) != NEST_OK) return st;
+    }
+    if ((st = nest_solver_set_dt_sequence(s, nullptr, 0, 2)) != NEST_OK) return st;
+    a->forward_done = true;
+    return NEST_OK;
+}
+
+nest_status nest_adjoint_backward(nest_adjoint* a, const void* lam_final, void* lam_initial, int on_device) {
+    if (!a) return fail(NEST_ERR_INVALID, "null adjoint handle");
+    if (!a->forward_done) return fail(NEST_ERR_INVALID, "run nest_adjoint_forward first");
+    if (!lam_final || !lam_initial) return fail(NEST_ERR_INVALID, "null adjoint buffer");
+    nest_solver* s = a->s;
+    size_t bytes = s->state_bytes();
+    nest_status st;
+    CK(cudaStreamSynchronize(s->st));
+    auto t0 = std::chrono::high_resolution_clock::now();
+    a->advanced = 0;
+    int cur = 0;
+    CK(cudaMemcpyAsync(a->lam[0], lam_final, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       s->st));
+    if (a->policy == NEST_CKPT_UNIFORM) {
+        int K = a->param;
+        int nseg = (a->nsteps + K - 1) / K;
+        for (int g = nseg - 1; g >= 0; --g) {
+            int j0 = g * K, j1 = std::min(a->nsteps, j0 + K);
+            if ((st = copy_state_dev(a, a->work, a->slots[g])) != NEST_OK) return st;
+            for (int j = j0; j < j1; ++j) {
+                if ((st = copy_state_dev(a, a->seg_un[j - j0], a->work)) != NEST_OK) return st;
+                cudaError_t e = a->stepper->stage1(a->work, a->seg_u1[j - j0], a->dts[j]);
+                if (e == cudaSuccess && j + 1 < j1) e = a->stepper->stage2(a->work, a->seg_u1[j - j0], a->dts[j]);
+                if (e != cudaSuccess) return cuda_fail(e, "segment recompute");
+                if (j + 1 < j1) ++a->advanced;
+            }
+            for (int j = j1 - 1; j >= j0; --j) {
+                cudaError_t e = a->stepper->adjoint_step(a->seg_un[j - j0], a->seg_u1[j - j0], a->dts[j],
+                                                         a->lam[cur], a->lam[cur ^ 1], a->tmp);
+                if (e != cudaSuccess) return cuda_fail(e, "adjoint step");
+                cur ^= 1;
+            }
+        }
+    } else {
+        if ((st = reverse_binomial(a, 0, a->nsteps, 0, a->param - 1, cur)) != NEST_OK) return st;
+    }
+    CK(cudaMemcpyAsync(lam_initial, a->lam[cur], bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       s->st));
+    CK(cudaStreamSynchronize(s->st));
+    auto t1 = std::chrono::high_resolution_clock::now();
+    a->bwd_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    return NEST_OK;
+}
+
+nest_status nest_adjoint_get_dts(nest_adjoint* a, double* dts) {
+    if (!a || !dts) return fail(NEST_ERR_INVALID, "null argument");
+    if (!a->forward_done) return fail(NEST_ERR_INVALID, "run nest_adjoint_forward first");
+    std::copy(a->dts.begin(), a->dts.end(), dts);
+    return NEST_OK;
+}
+
+nest_status nest_adjoint_stats(nest_adjoint* a, double* fwd_ms, double* bwd_ms, long long* recomputed_steps,
+                               long long* snapshot_bytes) {
+    if (!a) return fail(NEST_ERR_INVALID, "null adjoint handle");
+    if (fwd_ms) *fwd_ms = a->fwd_ms;
+    if (bwd_ms) *bwd_ms = a->bwd_ms;
+    if (recomputed_steps) *recomputed_steps = a->advanced;
+    if (snapshot_bytes) *snapshot_bytes = a->snap_bytes;
+    return NEST_OK;
+}
+
+}  // extern "C"

@@ -20,97 +20,32 @@
 #include <tuple>
 #include <vector>
 
-#include "../../include/nest_b200.h"
-#include "common.cuh"
-#include "euler2d_kernels.cuh"
-#include "kernels.h"
+#include "solver_impl.h"
 
 using namespace nestb;
+using namespace nestb::rt;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
-nest_status fail(nest_status st, const std::string& msg) {
+nest_status nestb::rt::fail(nest_status st, const std::string& msg) {
     g_last_error = msg;
     return st;
 }
 
-nest_status cuda_fail(cudaError_t e, const char* what) {
+nest_status nestb::rt::cuda_fail(cudaError_t e, const char* what) {
     return fail(e == cudaErrorMemoryAllocation ? NEST_ERR_OOM : NEST_ERR_CUDA,
                 std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-#define CK(call)                                              \
-    do {                                                      \
-        cudaError_t e__ = (call);                             \
-        if (e__ != cudaSuccess) return cuda_fail(e__, #call); \
-    } while (0)
-
-double bits_to_double(unsigned long long b) {
+double nestb::rt::bits_to_double(unsigned long long b) {
     double d;
     std::memcpy(&d, &b, sizeof d);
     return d;
 }
 
-constexpr int GRAPH_STEPS = 16;  // steps per captured graph (even: parity-neutral)
-
-struct GraphKey {
-    int nsteps, parity;
-    double cfl, t_final, fixed_dt;
-    int max_steps;
-    const double* dts_in;
-    double* dts_out;
-    int dts_cap, tx, warps;
-    bool operator<(const GraphKey& o) const {
-        return std::tie(nsteps, parity, cfl, t_final, fixed_dt, max_steps, dts_in, dts_out, dts_cap, tx, warps) <
-               std::tie(o.nsteps, o.parity, o.cfl, o.t_final, o.fixed_dt, o.max_steps, o.dts_in, o.dts_out,
-                        o.dts_cap, o.tx, o.warps);
-    }
-};
-
-}  // namespace
-
 nest_status nestb::record_error(nest_status st, const std::string& msg) { return fail(st, msg); }
-
-struct nest_solver {
-    nest_solver_desc d{};
-    int h = 2;
-    int n_total = 0;           // 1D: n + 2h
-    int pitch = 0;             // 2D: elements per row
-    long long vstride = 0;     // elements per variable plane
-    int nvars = 3;
-    size_t esize = 8;
-    void* U = nullptr;
-    void* U1 = nullptr;
-    StepCtrl* ctrl = nullptr;
-    StepCtrl* host_ctrl = nullptr;   // pinned mirror
-    double* partials = nullptr;
-    long long nrec = 0;
-    double* totals_dev = nullptr;
-    double* dts_in = nullptr;
-    double* dts_out = nullptr;
-    int dts_cap = 0;
-    int dts_mode = 2;
-    cudaStream_t st = nullptr;
-    bool own_stream = false;
-    int parity = 0;
-    bool prepared = false;
-    int tx = 64, warps = 4;
-    std::map<GraphKey, cudaGraphExec_t> graphs;
-
-    bool resident() const {
-        return d.dim == 1 && !(d.flags & NEST_FLAG_NO_RESIDENT) &&
-               resident_smem_bytes(d.nx, h) <= 220 * 1024;
-    }
-    Geo2D geo() const {
-        Geo2D g;
-        g.nx = d.nx; g.ny = d.ny; g.pitch = pitch; g.vstride = vstride;
-        g.bcx = d.bc_x; g.bcy = d.bc_y; g.dx = d.dx; g.dy = d.dy; g.gamma = d.gamma;
-        return g;
-    }
-    size_t state_bytes() const { return esize * (size_t)nvars * (size_t)vstride; }
-};
 
 namespace {
 
@@ -128,8 +63,10 @@ LoopParams base_params(const nest_solver* s) {
     return lp;
 }
 
+}  // namespace
+
 // Ghost fill + wave-speed maxima of the current state into slot `parity`.
-nest_status prepare(nest_solver* s) {
+nest_status nestb::rt::prepare(nest_solver* s) {
     CK(cudaMemsetAsync(&s->ctrl->maxs[s->parity][0], 0, 2 * sizeof(unsigned long long), s->st));
     cudaError_t e;
     if (s->d.dim == 1) {
@@ -145,10 +82,12 @@ nest_status prepare(nest_solver* s) {
 }
 
 // Enqueue one step (two kernels) with parity p; `which` selects the stages.
-cudaError_t enqueue_step(nest_solver* s, const LoopParams& lp, int p, int which = 3) {
+cudaError_t nestb::rt::enqueue_step(nest_solver* s, const LoopParams& lp, int p, int which) {
     if (s->d.dim == 1)
         return launch_1d_step((double*)s->U, (double*)s->U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp,
                               s->ctrl, p, which, s->st);
+    if (s->d.flags & NEST_FLAG_SPLIT_COMPAT)
+        return launch_2d_compat_step((double*)s->U, (double*)s->U1, s->geo(), lp, s->ctrl, p, which, s->st);
     if (s->d.precision == NEST_F64)
         return launch_2d_step_f64((double*)s->U, (double*)s->U1, s->geo(), lp, s->ctrl, s->partials, p, s->tx,
                                   s->warps, which, s->st);
@@ -158,6 +97,8 @@ cudaError_t enqueue_step(nest_solver* s, const LoopParams& lp, int p, int which 
     return launch_2d_step_f32x2((float*)s->U, (float*)s->U1, s->geo(), lp, s->ctrl, s->partials, p, s->tx,
                                 s->warps, (s->d.flags & NEST_FLAG_REPAIR) != 0, which, s->st);
 }
+
+namespace {
 
 // Enqueue nsteps steps of the tiled path; whole chunks go through cached graphs.
 nest_status enqueue_steps(nest_solver* s, int nsteps, const LoopParams& lp) {
@@ -198,12 +139,16 @@ nest_status enqueue_steps(nest_solver* s, int nsteps, const LoopParams& lp) {
     return NEST_OK;
 }
 
-nest_status read_ctrl(nest_solver* s) {
+}  // namespace
+
+nest_status nestb::rt::read_ctrl(nest_solver* s) {
     CK(cudaMemcpyAsync(s->host_ctrl, s->ctrl, sizeof(StepCtrl), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     if (s->host_ctrl->err & ERRW_NONFINITE) return fail(NEST_ERR_NUMERIC, "non-finite wave speed: the state blew up");
     return NEST_OK;
 }
+
+namespace {
 
 // Advance by at most `budget` steps (<= 0: unbounded) with the given loop
 // parameters; on the resident 1D path this is a single launch.
@@ -283,6 +228,10 @@ nest_status nest_solver_create(const nest_solver_desc* d, nest_solver** out) {
     if (d->dim == 1 && d->precision != NEST_F64) return fail(NEST_ERR_UNSUPPORTED, "1D solver is FP64");
     if (d->precision != NEST_F64 && d->precision != NEST_F32) return fail(NEST_ERR_INVALID, "bad precision");
     if (d->dim == 2 && (long long)d->nx * d->ny > (1ll << 31)) return fail(NEST_ERR_INVALID, "domain too large");
+    if ((d->flags & NEST_FLAG_SPLIT_COMPAT) && (d->dim != 2 || d->precision != NEST_F64))
+        return fail(NEST_ERR_UNSUPPORTED, "nest's split scheme runs in 2D FP64");
+    if ((d->flags & NEST_FLAG_SPLIT_COMPAT) && (d->flags & NEST_FLAG_TOTALS))
+        return fail(NEST_ERR_UNSUPPORTED, "totals are kept by the RK2 scheme only");
 
     nest_solver* s = new (std::nothrow) nest_solver;
     if (!s) return fail(NEST_ERR_OOM, "host allocation failed");
@@ -1013,6 +962,16 @@ nest_status nest_batch_totals(nest_batch* b, double* out) {
     CK(cudaStreamSynchronize(b->st));
     for (int p = 0; p < b->count; ++p)
         for (int k = 0; k < 4; ++k) out[4 * p + k] *= b->probs[p].g.dx * b->probs[p].g.dy;
+    return NEST_OK;
+}
+
+nest_status nest_batch_reset(nest_batch* b) {
+    nest_status r = batch_check(b);
+    if (r != NEST_OK) return r;
+    CK(cudaMemsetAsync(b->ctrls, 0, sizeof(StepCtrl) * b->count, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    b->parity = 0;
+    b->prepared = false;
     return NEST_OK;
 }
 

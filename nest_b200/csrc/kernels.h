@@ -39,6 +39,10 @@ cudaError_t launch_2d_step_f32x2(float* U, float* U1, const Geo2D& g, const Loop
                                  double* partials, int p, int tx, int warps, bool repair, int which,
                                  cudaStream_t st);
 
+// nest's split 2D scheme (x-sweep = stage 1, y-sweep = stage 2), FP64.
+cudaError_t launch_2d_compat_step(double* U, double* U1, const Geo2D& g, const LoopParams& lp, StepCtrl* ctrl, int p,
+                                  int which, cudaStream_t st);
+
 // Batched persistent stages (one launch per stage over the work list).
 template <typename T> struct BatchArgs;
 cudaError_t launch_batch_f64(const BatchArgs<double>& b, int which, int blocks, int warps, cudaStream_t st);

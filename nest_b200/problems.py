@@ -73,3 +73,31 @@ def kh_sizes(count: int = 512, seed: int = 0, lo: int = 64, hi: int = 1024, step
     rng = np.random.default_rng(seed)
     choices = np.arange(lo, hi + 1, step)
     return rng.choice(choices, size=count), rng.choice(choices, size=count)
+
+
+def fourier_fields_1d(n: int, seed: int, modes: int = 16):
+    """Primitive fields of the 1D adjoint workload on [0,1) (periodic, n cells):
+    f, g, h = sum_{k=1..modes} (a_k cos 2 pi k x + b_k sin 2 pi k x) with
+    a, b ~ N(0, 1) (numpy PCG64, `seed`), scaled to rho = 1 + 0.5 f/max|f|,
+    u = 0.3 g/max|g|, p = 1 + 0.5 h/max|h|."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(n) + 0.5) / n
+    k = np.arange(1, modes + 1)[:, None]
+    out = []
+    for _ in range(3):
+        a, b = rng.standard_normal((2, modes, 1))
+        f = (a * np.cos(2 * np.pi * k * x) + b * np.sin(2 * np.pi * k * x)).sum(axis=0)
+        out.append(f / np.abs(f).max())
+    f, g, h = out
+    return 1.0 + 0.5 * f, 0.3 * g, 1.0 + 0.5 * h
+
+
+def prim_to_cons_1d(rho, u, p, gamma: float = GAMMA, h: int = 2) -> np.ndarray:
+    """(rho, u, p) interior fields -> conserved SoA [3][n + 2h] (ghosts zero;
+    the solver fills them)."""
+    n = len(rho)
+    U = np.zeros((3, n + 2 * h))
+    U[0, h:h + n] = rho
+    U[1, h:h + n] = rho * u
+    U[2, h:h + n] = p / (gamma - 1.0) + 0.5 * rho * u * u
+    return U

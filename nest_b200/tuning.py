@@ -88,6 +88,35 @@ def best_tiling(form: str, nx: int, ny: int, tune_if_missing: bool = True):
     return DEFAULT[form]
 
 
+def best_batch_tiling(batch, nx, ny, steps: int = 4, save: bool = True):
+    """Cached (rows per item, warps per block, blocks per SM) for a batch of
+    these sizes on this device; sweeps the candidates on the batch itself
+    (its state is advanced by the sweep: call before uploading)."""
+    import hashlib
+    key = f"{_device_key()}|batch|{hashlib.sha1(np.asarray([nx, ny]).tobytes()).hexdigest()[:12]}|{len(nx)}"
+    cache = _load()
+    if key in cache:
+        e = cache[key]
+        return int(e["rows_per_tile"]), int(e["warps_per_block"]), int(e["blocks_per_sm"])
+    times = {}
+    for r in (16, 32, 64):
+        for w in (1, 2, 4):
+            for bps in (0, 4):
+                batch.set_tiling(r, w, bps)
+                batch.step_profiled(1, 0.4)
+                _, _, tot = batch.step_profiled(steps, 0.4)
+                times[(r, w, bps)] = tot / steps
+    best = min(times, key=times.get)
+    if save:
+        cache[key] = {"rows_per_tile": best[0], "warps_per_block": best[1], "blocks_per_sm": best[2],
+                      "ms_per_step": times[best]}
+        try:
+            CACHE.write_text(json.dumps(cache, indent=1, sort_keys=True))
+        except OSError:
+            pass
+    return best
+
+
 if __name__ == "__main__":
     import argparse
 

@@ -6,6 +6,8 @@ by oracle/Makefile from the nest source tree).  Outputs, all small:
                         periodic Sod, N=100, t=0.1, CFL 0.3, SoA 3 x 104
   sod1d_final.npy       last output of the sod1d example (examples/sod1d/sod1d.cpp):
                         columns x rho u p e at t=0.2, N=400, 4 periodic patches
+  sod2d_final.npz       last output of the sod2d example (examples/sod2d/sod2d.cpp):
+                        columns x y rho u v p at t=0.2, 200 x 20 cells, 2 x 2 periodic patches
   known_answers.json    nest's numerics on the inputs of tests/test_euler.cpp:54-237
                         and on a seeded set of random states
 
@@ -41,6 +43,18 @@ def main():
         assert rc == 0, rc
         last = sorted(glob.glob(os.path.join(td, "sod_*.dat")))[-1]
         np.save(HERE / "sod1d_final.npy", np.loadtxt(last, comments="#"))
+
+    with tempfile.TemporaryDirectory() as td:
+        os.chdir(td)
+        try:
+            rc = ref.L.ref_sod2d_main()
+        finally:
+            os.chdir(cwd)
+        assert rc == 0, rc
+        outs = sorted(f for f in glob.glob(os.path.join(td, "sod2d_*.dat")) if "xslice" not in f)
+        a = np.loadtxt(outs[-1], comments="#").astype(np.float64)
+        np.savez_compressed(HERE / "sod2d_final.npz", x=a[:, 0], y=a[:, 1], rho=a[:, 2], u=a[:, 3], v=a[:, 4],
+                            p=a[:, 5])
 
     import ctypes as C
     dp = C.POINTER(C.c_double)

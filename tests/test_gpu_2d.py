@@ -170,3 +170,25 @@ def test_fp32_packed_matches_fp64_and_scalar(gpu, nx, ny, bc):
         assert np.array_equal(G[:, 2:-2, 0], G[:, 2:-2, 2]) and np.array_equal(G[:, 2:-2, -1], G[:, 2:-2, -3])
     else:
         assert np.array_equal(G[:, 2:-2, 0], G[:, 2:-2, ny]) and np.array_equal(G[:, 2:-2, -1], G[:, 2:-2, 3])
+
+
+def test_split_compat_matches_nest_sweeps(gpu, oracle, ref):
+    """nest's own 2D scheme on the device (NEST_FLAG_SPLIT_COMPAT): the sod2d
+    configuration (200 x 20, 2 x 2 periodic patches, CFL 0.3, t = 0.2) equals
+    nest's x_sweep_t / y_sweep_t run on the CPU bit for bit."""
+    from test_oracle import sod2d_reference_run
+    want, t_ref, steps_ref = sod2d_reference_run(ref, oracle)
+    nx, ny = 200, 20
+    from nest_b200.problems import prim_to_cons_2d
+    x = (np.arange(-2, nx + 2) + 0.5) / nx
+    X = np.repeat(x[:, None], ny + 4, axis=1)
+    left = X < 0.5
+    z = np.zeros_like(X)
+    U = prim_to_cons_2d(np.where(left, 1.0, 0.125), z, z, np.where(left, 1.0, 0.1))
+    s = gpu.Solver(2, nx, ny, dx=1.0 / nx, dy=0.1 / ny, bc=BC_PERIODIC, precision=gpu.F64,
+                   flags=gpu.FLAG_SPLIT_COMPAT)
+    s.upload(U)
+    steps = s.run_to(0.2, 0.3)
+    got = s.download()
+    assert steps == steps_ref and s.time()[0] == t_ref
+    assert np.array_equal(got[:, 2:-2, 2:-2], want[:, 2:-2, 2:-2])
