@@ -55,10 +55,24 @@ class Adjoint:
         check(lib.nest_adjoint_forward(self._h, cfl, p), "nest_adjoint_forward")
 
     def backward(self, lam_final: np.ndarray) -> np.ndarray:
-        """Host arrays in the solver's extended layout."""
-        lam_final = np.ascontiguousarray(lam_final, dtype=np.float64)
+        """Adjoint of the final state -> adjoint of the initial state, as host
+        arrays in the solver's extended layout (1D [3][n+2h], 2D [4][nx+4][ny+4])."""
+        s = self.solver
+        lam_final = np.ascontiguousarray(lam_final, dtype=s.dtype)
+        if s.dim == 1:
+            out = np.zeros_like(lam_final)
+            check(lib.nest_adjoint_backward(self._h, lam_final.ctypes.data, out.ctypes.data, 0), "nest_adjoint_backward")
+            return out
+        _, pitch, vs = s.state_ptr()
+        rows = s.nx + 4
+        dev = np.zeros(4 * vs, dtype=s.dtype)
+        for k in range(4):
+            dev[k * vs:k * vs + rows * pitch].reshape(rows, pitch)[:, :s.ny + 4] = lam_final[k]
+        res = np.zeros_like(dev)
+        check(lib.nest_adjoint_backward(self._h, dev.ctypes.data, res.ctypes.data, 0), "nest_adjoint_backward")
         out = np.zeros_like(lam_final)
-        check(lib.nest_adjoint_backward(self._h, lam_final.ctypes.data, out.ctypes.data, 0), "nest_adjoint_backward")
+        for k in range(4):
+            out[k] = res[k * vs:k * vs + rows * pitch].reshape(rows, pitch)[:, :s.ny + 4]
         return out
 
     def backward_device(self, lam_final_ptr: int, lam_initial_ptr: int):

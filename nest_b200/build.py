@@ -35,6 +35,7 @@ UNITS = {
     "adjoint1d.cu": [],
     "adjoint.cpp": ["-x", "cu"],
     "exchange.cu": [],
+    "adjoint2d.cu": [],
 }
 
 

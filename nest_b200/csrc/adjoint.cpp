@@ -77,6 +77,48 @@ struct Stepper1D : Stepper {
     }
 };
 
+// 2D solver (FP64 plain form or FP32 form): the stage kernels are the
+// solver's own; the FP32 form's state is advanced by the packed kernel.
+struct Stepper2D : Stepper {
+    nest_solver* s;
+    StepCtrl* ctrl;
+    Stepper2D(nest_solver* s_, StepCtrl* c) : s(s_), ctrl(c) {}
+    LoopParams lp(double dt) const {
+        LoopParams p{};
+        p.cfl = 1.0;
+        p.fixed_dt = dt;
+        return p;
+    }
+    cudaError_t run(void* U, void* U1, double dt, int which) {
+        if (s->d.precision == NEST_F64)
+            return launch_2d_step_f64((double*)U, (double*)U1, s->geo(), lp(dt), ctrl, nullptr, 0, s->tx, s->warps,
+                                      which, s->st);
+        return launch_2d_step_f32x2((float*)U, (float*)U1, s->geo(), lp(dt), ctrl, nullptr, 0, s->tx, s->warps,
+                                    (s->d.flags & NEST_FLAG_REPAIR) != 0, which, s->st);
+    }
+    cudaError_t step(void* U, void* U1, double dt) override { return run(U, U1, dt, 3); }
+    cudaError_t stage1(void* U, void* U1, double dt) override { return run(U, U1, dt, 1); }
+    cudaError_t stage2(void* U, void* U1, double dt) override { return run(U, U1, dt, 2); }
+    cudaError_t adjoint_step(void* Un, void* U1, double dt, void* lam, void* lam_new, void* tmp) override {
+        double lx = dt / s->d.dx, ly = dt / s->d.dy;
+        cudaError_t e;
+        if (s->d.precision == NEST_F64) {
+            e = launch_2d_adjoint_stage_f64((const double*)U1, (const double*)lam, nullptr, (double*)tmp, s->geo(), lx,
+                                            ly, 0.5, 0.0, s->st);
+            if (e == cudaSuccess)
+                e = launch_2d_adjoint_stage_f64((const double*)Un, (const double*)tmp, (const double*)lam,
+                                                (double*)lam_new, s->geo(), lx, ly, 1.0, 0.5, s->st);
+        } else {
+            e = launch_2d_adjoint_stage_f32((const float*)U1, (const float*)lam, nullptr, (float*)tmp, s->geo(), lx,
+                                            ly, 0.5, 0.0, s->st);
+            if (e == cudaSuccess)
+                e = launch_2d_adjoint_stage_f32((const float*)Un, (const float*)tmp, (const float*)lam,
+                                                (float*)lam_new, s->geo(), lx, ly, 1.0, 0.5, s->st);
+        }
+        return e;
+    }
+};
+
 long long binom(int n, int k) {  // C(n, k), saturating
     if (k < 0 || k > n) return 0;
     long double r = 1;
@@ -200,9 +242,11 @@ nest_status nest_adjoint_create(nest_solver* s, int nsteps, int policy, int para
     if (nsteps <= 0) return fail(NEST_ERR_INVALID, "nsteps must be positive");
     if (policy != NEST_CKPT_UNIFORM && policy != NEST_CKPT_BINOMIAL) return fail(NEST_ERR_INVALID, "bad policy");
     if (param < 1) return fail(NEST_ERR_INVALID, "checkpoint parameter must be >= 1");
-    if (s->d.dim != 1 || s->d.precision != NEST_F64)
-        return fail(NEST_ERR_UNSUPPORTED, "adjoint: this build supports the 1D FP64 solver");
-    if (s->d.bc_x != NEST_BC_PERIODIC) return fail(NEST_ERR_UNSUPPORTED, "adjoint: periodic boundaries");
+    if (s->d.dim == 1 && s->d.precision != NEST_F64) return fail(NEST_ERR_UNSUPPORTED, "adjoint: 1D runs in FP64");
+    if (s->d.bc_x != NEST_BC_PERIODIC || (s->d.dim == 2 && s->d.bc_y != NEST_BC_PERIODIC))
+        return fail(NEST_ERR_UNSUPPORTED, "adjoint: periodic boundaries");
+    if (s->d.flags & (NEST_FLAG_SPLIT_COMPAT | NEST_FLAG_FP32_SCALAR))
+        return fail(NEST_ERR_UNSUPPORTED, "adjoint: unsplit RK2 scheme only");
     auto* a = new (std::nothrow) nest_adjoint;
     if (!a) return fail(NEST_ERR_OOM, "host allocation failed");
     a->s = s;
@@ -213,7 +257,8 @@ nest_status nest_adjoint_create(nest_solver* s, int nsteps, int policy, int para
     cudaError_t e = cudaMalloc(&a->ctrl, sizeof(StepCtrl));
     if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(ctrl)"));
     if ((e = cudaMemset(a->ctrl, 0, sizeof(StepCtrl))) != cudaSuccess) return cleanup(cuda_fail(e, "memset"));
-    a->stepper.reset(new Stepper1D(s, a->ctrl));
+    if (s->d.dim == 1) a->stepper.reset(new Stepper1D(s, a->ctrl));
+    else a->stepper.reset(new Stepper2D(s, a->ctrl));
     nest_status st;
     int nslots = policy == NEST_CKPT_UNIFORM ? (nsteps + a->param - 1) / a->param : a->param;
     a->slots.assign(nslots, nullptr);

@@ -43,6 +43,14 @@ cudaError_t launch_2d_step_f32x2(float* U, float* U1, const Geo2D& g, const Loop
 cudaError_t launch_2d_compat_step(double* U, double* U1, const Geo2D& g, const LoopParams& lp, StepCtrl* ctrl, int p,
                                   int which, cudaStream_t st);
 
+// Adjoint of one 2D stage: Lin = alpha * adj(U, Lout) + beta * Extra (periodic).
+cudaError_t launch_2d_adjoint_stage_f64(const double* U, const double* Lout, const double* Extra, double* Lin,
+                                        const Geo2D& g, double lx, double ly, double alpha, double beta,
+                                        cudaStream_t st);
+cudaError_t launch_2d_adjoint_stage_f32(const float* U, const float* Lout, const float* Extra, float* Lin,
+                                        const Geo2D& g, double lx, double ly, double alpha, double beta,
+                                        cudaStream_t st);
+
 // Batched persistent stages (one launch per stage over the work list).
 template <typename T> struct BatchArgs;
 cudaError_t launch_batch_f64(const BatchArgs<double>& b, int which, int blocks, int warps, cudaStream_t st);

@@ -124,3 +124,79 @@ def tangent_rollout(U0, dU0, dts, dx, gamma=1.4):
     for dt in dts:
         U = heun(gamma, U, dt / dx)
     return ([[U[i][k].v for i in range(n)] for k in range(3)], [[U[i][k].d for i in range(n)] for k in range(3)])
+
+
+# ---------------------------------------------------------------------------
+# 2D unsplit stage (oracle/euler_oracle.c: orc2d_stage / orc_hlle2d), periodic
+# ---------------------------------------------------------------------------
+
+def ke2(r, u, v):
+    return 0.5 * r * u * u + 0.5 * r * v * v
+
+
+def prim2(g, U):
+    r, mu, mv, E = U
+    u, v = mu / r, mv / r
+    p = (g - 1.0) * (E - ke2(r, u, v))
+    return [r, u, v, D(0.0) if p.v < 0.0 else p]
+
+
+def hlle2(g, WL, WR):  # (rho, un, ut, p) -> (rho un, rho un un + p, rho un ut, (E + p) un)
+    rL, nL, tL, pL = WL
+    rR, nR, tR, pR = WR
+    cL, cR = dsqrt(g * pL / rL), dsqrt(g * pR / rR)
+    EL = pL / (g - 1.0) + ke2(rL, nL, tL)
+    ER = pR / (g - 1.0) + ke2(rR, nR, tR)
+    SL = smin(nL - cL, nR - cR)
+    SR = smax(nL + cL, nR + cR)
+    FL = [rL * nL, rL * nL * nL + pL, rL * nL * tL, (EL + pL) * nL]
+    FR = [rR * nR, rR * nR * nR + pR, rR * nR * tR, (ER + pR) * nR]
+    UL = [rL, rL * nL, rL * tL, EL]
+    UR = [rR, rR * nR, rR * tR, ER]
+    if SL.v >= 0.0:
+        return FL
+    if SR.v <= 0.0:
+        return FR
+    return [(SR * FL[k] - SL * FR[k] + SL * SR * (UR[k] - UL[k])) / (SR - SL) for k in range(4)]
+
+
+def stage2d(g, U, lx, ly):
+    """U[i][j] = [rho, mu, mv, E] duals on an nx x ny periodic grid."""
+    nx, ny = len(U), len(U[0])
+    W = [[prim2(g, U[i][j]) for j in range(ny)] for i in range(nx)]
+
+    def face(a2, a, b, b2, xdir):
+        perm = (lambda w: [w[0], w[1], w[2], w[3]]) if xdir else (lambda w: [w[0], w[2], w[1], w[3]])
+        A2, A, B, B2 = perm(a2), perm(a), perm(b), perm(b2)
+        L = [A[k] + 0.5 * minmod(A[k] - A2[k], B[k] - A[k]) for k in range(4)]
+        R = [B[k] - 0.5 * minmod(B[k] - A[k], B2[k] - B[k]) for k in range(4)]
+        f = hlle2(g, L, R)
+        return [f[0], f[1], f[2], f[3]] if xdir else [f[0], f[2], f[1], f[3]]
+
+    out = []
+    for i in range(nx):
+        row = []
+        for j in range(ny):
+            w = lambda a, b: W[a % nx][b % ny]
+            fxm = face(w(i - 2, j), w(i - 1, j), w(i, j), w(i + 1, j), True)
+            fxp = face(w(i - 1, j), w(i, j), w(i + 1, j), w(i + 2, j), True)
+            fym = face(w(i, j - 2), w(i, j - 1), w(i, j), w(i, j + 1), False)
+            fyp = face(w(i, j - 1), w(i, j), w(i, j + 1), w(i, j + 2), False)
+            row.append([U[i][j][k] - (lx * (fxp[k] - fxm[k]) + ly * (fyp[k] - fym[k])) for k in range(4)])
+        out.append(row)
+    return out
+
+
+def tangent_rollout_2d(U0, dU0, dts, dx, dy, gamma=1.4):
+    """U0, dU0: arrays [4][nx][ny] (interior, periodic).  Heun steps with the
+    given dts; returns (U_T, dU_T) as numpy-convertible nested lists [4][nx][ny]."""
+    nx, ny = len(U0[0]), len(U0[0][0])
+    U = [[[D(U0[k][i][j], dU0[k][i][j]) for k in range(4)] for j in range(ny)] for i in range(nx)]
+    for dt in dts:
+        lx, ly = dt / dx, dt / dy
+        U1 = stage2d(gamma, U, lx, ly)
+        U2 = stage2d(gamma, U1, lx, ly)
+        U = [[[0.5 * (U[i][j][k] + U2[i][j][k]) for k in range(4)] for j in range(ny)] for i in range(nx)]
+    val = [[[U[i][j][k].v for j in range(ny)] for i in range(nx)] for k in range(4)]
+    der = [[[U[i][j][k].d for j in range(ny)] for i in range(nx)] for k in range(4)]
+    return val, der

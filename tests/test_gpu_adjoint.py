@@ -133,3 +133,92 @@ def test_autograd_rollout(gpu):
     fd = (L(1e-6) - L(-1e-6)) / 2e-6
     ad = float(np.sum(rho.grad.cpu().numpy() * dr))
     assert abs(ad - fd) <= 1e-6 * abs(fd), (ad, fd)
+
+
+def adjoint2d_case(gpu, nx, ny, nsteps, prec, seed=3, policy=0, param=8):
+    from nest_b200.adjoint import Adjoint
+    from nest_b200.problems import kelvin_helmholtz
+    U0 = kelvin_helmholtz(nx, ny, seed=seed)
+    dt = np.float64 if prec == gpu.F64 else np.float32
+    s = gpu.Solver(2, nx, ny, bc=gpu.BC_PERIODIC, precision=prec)
+    s.upload(U0.astype(dt))
+    adj = Adjoint(s, nsteps, policy, param)
+    adj.forward(0.4)
+    return U0, s, adj
+
+
+def test_adjoint2d_equals_exact_tangent(gpu):
+    from oracle.tangent import tangent_rollout_2d
+    nx, ny, nsteps = 12, 10, 3
+    U0, s, adj = adjoint2d_case(gpu, nx, ny, nsteps, gpu.F64)
+    dts = adj.dts()
+    UT = s.download()
+    rng = np.random.default_rng(2)
+    w = rng.standard_normal((4, nx, ny))
+    lamT = np.zeros_like(UT)
+    lamT[:, 2:-2, 2:-2] = w
+    lam0 = adj.backward(lamT)
+    for _ in range(2):
+        d = rng.standard_normal((4, nx, ny))
+        val, der = tangent_rollout_2d(U0[:, 2:-2, 2:-2], d, dts, 1.0 / nx, 1.0 / ny)
+        assert np.array_equal(np.array(val), UT[:, 2:-2, 2:-2])
+        jvp = float(np.sum(w * np.array(der)))
+        vjp = float(np.sum(lam0[:, 2:-2, 2:-2] * d))
+        assert abs(jvp - vjp) <= 1e-11 * max(1.0, abs(jvp)), (jvp, vjp)
+
+
+def ke_v_loss_and_lambda(U, nx, ny):
+    """L = integral of 1/2 rho v^2 dA and its gradient w.r.t. (rho, mu, mv, E)."""
+    r, mv = U[0, 2:-2, 2:-2].astype(np.float64), U[2, 2:-2, 2:-2].astype(np.float64)
+    v = mv / r
+    dA = 1.0 / (nx * ny)
+    lam = np.zeros(U.shape)
+    lam[0, 2:-2, 2:-2] = -0.5 * v * v * dA
+    lam[2, 2:-2, 2:-2] = v * dA
+    return 0.5 * np.sum(r * v * v) * dA, lam
+
+
+def test_adjoint2d_finite_differences_fp64(gpu):
+    nx, ny, nsteps = 48, 40, 30
+    U0, s, adj = adjoint2d_case(gpu, nx, ny, nsteps, gpu.F64, seed=4)
+    dts = adj.dts()
+    L0, lamT = ke_v_loss_and_lambda(s.download(), nx, ny)
+    lam0 = adj.backward(lamT)
+    rng = np.random.default_rng(8)
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    X, Y = np.meshgrid(x, y, indexing="ij")
+
+    def L(U):
+        s2 = gpu.Solver(2, nx, ny, bc=gpu.BC_PERIODIC, precision=gpu.F64)
+        s2.freeze_dts(dts)
+        s2.upload(U)
+        s2.step(nsteps, 0.4)
+        return ke_v_loss_and_lambda(s2.download(), nx, ny)[0]
+
+    for _ in range(4):
+        d = np.zeros_like(U0)
+        for k in range(4):
+            a, b, c = rng.standard_normal(3)
+            d[k, 2:-2, 2:-2] = a * np.sin(2 * np.pi * (X + b)) * np.cos(2 * np.pi * (2 * Y + c))
+        eps = 1e-8
+        fd = (L(U0 + eps * d) - L(U0 - eps * d)) / (2 * eps)
+        ad = float(np.sum(lam0[:, 2:-2, 2:-2] * d[:, 2:-2, 2:-2]))
+        assert abs(ad - fd) <= 1e-6 * abs(fd) + 1e-15, (ad, fd)
+
+
+def test_adjoint2d_fp32_vs_fp64(gpu):
+    """Gradient of the v kinetic energy w.r.t. the initial v field: FP32
+    forward + adjoint against the FP64 adjoint (binomial checkpointing)."""
+    nx = ny = 64
+    out = {}
+    for prec in (gpu.F64, gpu.F32):
+        U0, s, adj = adjoint2d_case(gpu, nx, ny, 40, prec, seed=5, policy=1, param=6)
+        _, lamT = ke_v_loss_and_lambda(s.download(), nx, ny)
+        lam0 = adj.backward(lamT).astype(np.float64)
+        r0 = U0[0, 2:-2, 2:-2]
+        v0 = U0[2, 2:-2, 2:-2] / r0
+        out[prec] = lam0[2, 2:-2, 2:-2] * r0 + lam0[3, 2:-2, 2:-2] * r0 * v0  # dL/dv0
+    g64, g32 = out[gpu.F64], out[gpu.F32]
+    rel = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
+    assert rel < 1e-3, rel
