@@ -15,9 +15,11 @@ Arms
                     cores (the oracle port: nest has no 2D RK2), one bounded
                     sample per step.  Rank 0 only.
 
-Multi-GPU (torchrun): every rank advances its own copy of the workload
-(replicas; the single-domain path has no data-path collective here), timing
-is the max over ranks, value is the sum over ranks.
+Multi-GPU (torchrun, N ranks): one domain of (N*4096) x 4096 cells cut into
+N x-slabs of 4096 x 4096, one per GPU (weak scaling): every step max-reduces
+the two wave-speed words over NCCL and swaps two ghost rows with each
+neighbour before each stage (nest_b200/shard.py).  Timing is the max over
+ranks; value counts every rank's cells.
 """
 from __future__ import annotations
 
@@ -54,6 +56,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--tiling", default="", help="rows,warps: fixed launch shape instead of the tuned one")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched-KH and adjoint measurements")
+    ap.add_argument("--slab-path", action="store_true",
+                    help="drive the domain through the x-slab driver even on one GPU (a one-rank group)")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=500)
     ap.add_argument("--adjoint-n", type=int, default=65536)
@@ -73,15 +77,21 @@ def peaks():
 # distributed plumbing
 # ---------------------------------------------------------------------------
 
-def dist_setup():
+def dist_setup(force: bool = False):
     import torch
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
+    if ws > 1 or force:
+        if ws == 1:
+            os.environ.setdefault("RANK", "0")
+            os.environ.setdefault("WORLD_SIZE", "1")
+            os.environ.setdefault("MASTER_PORT", "29531")
         import datetime
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
         dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
                                 timeout=datetime.timedelta(seconds=120))
     return ws, rank, local
@@ -196,6 +206,88 @@ def traffic_from_profiles(form: str, n: int):
     return {k: v * (n * n) / float(e["cells"]) for k, v in e["bytes_per_launch"].items()}
 
 
+def run_slabs(args, ws, rank, form, cfl, st):
+    """N>1: this rank's x-slab of the (ws*n) x n domain.  Returns the timed
+    figures of one form (same keys as the one-domain path)."""
+    import torch
+    import torch.distributed as dist
+    import nest_b200 as nb
+    from nest_b200.problems import riemann_2d
+    from nest_b200.shard import gpu_domain
+    from nest_b200.tuning import best_tiling
+    n = args.n
+    prec = nb.F32 if form == "f32" else nb.F64
+    dom, ranges = gpu_domain(ws * n, n, bc=nb.BC_OUTFLOW, precision=prec, group=dist.group.WORLD)
+    (slab,), ((x0, nl),) = dom.slabs, ranges
+    U = riemann_2d(ws * n, n, rows=(x0, nl))
+    U = U.astype(np.float32) if form == "f32" else U
+    tiling = tuple(int(v) for v in args.tiling.split(",")) if args.tiling else best_tiling(form, nl, n)
+    slab.solver.set_tiling(*tiling)
+    sst = slab.stream_obj
+    slab.solver.upload(U)
+    dom.step(args.warmup, cfl)
+    slab.solver.sync()
+    slab.solver.upload(U)
+    slab.solver.reset_time()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    e0.record(sst)
+    dom.step(args.steps, cfl)
+    e1.record(sst)
+    e1.synchronize()
+    t1 = time.time()
+    barrier(ws)
+    ms = allmax(ws, e0.elapsed_time(e1)) / args.steps
+    tsim, nst = slab.solver.time()
+    # per-kernel durations: the same steps again with events around each stage
+    slab.solver.upload(U)
+    slab.solver.reset_time()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    with slab.stream():
+        for k in range(args.steps):
+            dom.reduce_speeds()
+            dom.exchange(0)
+            ev[k][0].record(sst)
+            slab.stage(1, cfl, 0.0)
+            ev[k][1].record(sst)
+            dom.exchange(1)
+            ev[k][2].record(sst)
+            slab.stage(2, cfl, 0.0)
+            ev[k][3].record(sst)
+    sst.synchronize()
+    k1 = [e[0].elapsed_time(e[1]) for e in ev]
+    k2 = [e[2].elapsed_time(e[3]) for e in ev]
+    out = {"ms": ms, "k1": k1, "k2": k2, "tsim": tsim, "steps": nst, "tiling": tiling, "window": (t0, t1),
+           "cells_local": nl * n, "graph_ms": None}
+    if not args.no_e2e:
+        tdt = torch.float32 if form == "f32" else torch.float64
+        hin = torch.empty(U.shape, dtype=tdt, pin_memory=True)
+        hin.numpy()[...] = U
+        hout = torch.empty(U.shape, dtype=tdt, pin_memory=True)
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0.record(sst)
+        nb.solver.check(nb._capi.lib.nest_solver_upload(slab.solver._h, hin.data_ptr(), nb.LAYOUT_EXTENDED), "upload")
+        slab.solver.reset_time()
+        dom.step(args.steps, cfl)
+        nb.solver.check(nb._capi.lib.nest_solver_download(slab.solver._h, hout.data_ptr(), nb.LAYOUT_EXTENDED),
+                        "download")
+        slab.solver.time()
+        e1.record(sst)
+        e1.synchronize()
+        ems = allmax(ws, e0.elapsed_time(e1))
+        out["e2e"] = {"value": ws * nl * n * 2 * args.steps / (ems * 1e-3), "unit": UNIT, "ms_total": ems,
+                      "h2d_bytes_per_step": U.nbytes / args.steps, "d2h_bytes_per_step": (U.nbytes + 32) / args.steps,
+                      "api": "nest_solver_upload -> SlabDomain.step -> nest_solver_download -> nest_solver_time"}
+    barrier(ws)
+    torch.cuda.synchronize()
+    for sl in dom.slabs:
+        sl.solver.close()
+    return out
+
+
 def run_ours(args, ws, rank, local):
     import torch
     import nest_b200 as nb
@@ -208,7 +300,7 @@ def run_ours(args, ws, rank, local):
     cfl = 0.4
     hbm, peak_kind = peaks()
     st = torch.cuda.Stream()
-    U64 = riemann_2d(n, n)
+    U64 = riemann_2d(n, n) if ws == 1 and not args.slab_path else None
     results = {}
     clocks = ClockSampler(local)
     clocks.start()
@@ -216,6 +308,29 @@ def run_ours(args, ws, rank, local):
     forms = [f.strip() for f in args.forms.split(",") if f.strip()]
     launches = 0
     for form in forms:
+        if ws > 1 or args.slab_path:
+            r = run_slabs(args, ws, rank, form, cfl, st)
+            launches += 2 * args.steps
+            ab = alg_bytes_per_cell(form)
+            m1, m2 = float(np.mean(r["k1"])), float(np.mean(r["k2"]))
+            dom, dom_ms = ("stage2", m2) if m2 >= m1 else ("stage1", m1)
+            cl = r["cells_local"]
+            achieved = ab[dom] * cl / (dom_ms * 1e-3) / 1e9
+            tr = traffic_from_profiles(form, n)
+            value = ws * cl * 2 / (r["ms"] * 1e-3)
+            results[form] = {
+                "value": value, "ms_per_step": r["ms"], "sim_time": r["tsim"], "steps": r["steps"],
+                "tiling": {"rows_per_tile": r["tiling"][0], "warps_per_block": r["tiling"][1]},
+                "kernel_ms": {"stage1": m1, "stage2": m2},
+                "hbm_gbs_step": value / ws * ab["per_cell_update"] / 1e9,
+                "roofline": {"bound": "hbm", "kernel": f"k2d_{form}<{dom[-1]}>", "achieved": achieved, "peak": hbm,
+                             "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+                             "alg_bytes_per_launch": ab[dom] * cl, "traffic": (tr or {}).get(dom)},
+                "window": r["window"],
+            }
+            if "e2e" in r:
+                results[form]["e2e"] = r["e2e"]
+            continue
         prec = nb.F32 if form == "f32" else nb.F64
         U = U64.astype(np.float32) if form == "f32" else U64
         s = nb.Solver(2, n, n, bc=nb.BC_OUTFLOW, precision=prec, stream=st.cuda_stream)
@@ -278,9 +393,11 @@ def run_ours(args, ws, rank, local):
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": head, "data": "synthetic",
-        "config": {"workload": f"riemann2d {n}x{n} {head}", "nx": n, "ny": n,
+        "config": {"workload": f"riemann2d {ws * n}x{n} {head}", "nx": ws * n, "ny": n,
                    "patches": f"{n // 256}x{n // 256} of 256^2" if n % 256 == 0 else "one",
-                   "bc": "outflow", "cfl": cfl, "gamma": 1.4, "parallelism": f"replicas x{ws}",
+                   "bc": "outflow", "cfl": cfl, "gamma": 1.4,
+                   "parallelism": "one GPU" if ws == 1 and not args.slab_path else
+                   f"{ws} x-slabs of {n}x{n} (NCCL halo rows + wave-speed all-reduce)",
                    "l2": "inputs larger than L2 (two state buffers of %.0f MB each)" % (
                        4 * (n + 4) ** 2 * (4 if head == "f32" else 8) / 1e6)},
         "roofline": r["roofline"],
@@ -477,11 +594,14 @@ def main():
             return 0
         print(json.dumps(run_reference(args, rank)), flush=True)
         return 0
-    ws, rank, local = dist_setup()
+    ws, rank, local = dist_setup(args.slab_path)
+    if ws > 1 or args.slab_path:
+        import torch
+        torch.cuda.set_device(local)
     out = run_ours(args, ws, rank, local)
     if rank == 0:
         print(json.dumps(out), flush=True)
-    if ws > 1:
+    if ws > 1 or args.slab_path:
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0

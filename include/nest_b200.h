@@ -143,6 +143,22 @@ nest_status nest_solver_set_tiling(nest_solver* s, int rows_per_tile, int warps_
  * next n dts (read back with nest_solver_get_dts), mode 2 clears. */
 nest_status nest_solver_set_dt_sequence(nest_solver* s, const double* dts, int n, int mode);
 nest_status nest_solver_get_dts(nest_solver* s, double* dts, int n);
+/* Sharded domains (x-slabs on several GPUs).  xlo / xhi = 1 marks an x side
+ * whose two ghost rows a halo exchange fills: the kernels then neither write
+ * nor derive them.  Steps are driven stage by stage: before stage 1 the caller
+ * max-reduces the two wave-speed words of nest_solver_speed_slot across ranks
+ * (uint64 bit patterns of non-negative doubles, MAX) and fills the exchange
+ * ghost rows of the state (nest_solver_state_ptr); before stage 2 those of
+ * the stage buffer (nest_solver_stage_ptr, same pitch and plane stride).
+ * Row i of plane v starts at element v * vstride + (i + 2) * pitch. */
+nest_status nest_solver_set_exchange_sides(nest_solver* s, int xlo, int xhi);
+/* Enqueue one stage (1 or 2) of the current step; stage 2 ends the step.
+ * t_final > 0 clips dt to reach it; a step that would start at or past it is a no-op. */
+nest_status nest_solver_stage(nest_solver* s, int which, double cfl, double t_final);
+/* Device address of the current step's two wave-speed words. */
+nest_status nest_solver_speed_slot(nest_solver* s, void** dev);
+nest_status nest_solver_stage_ptr(nest_solver* s, void** dev);
+nest_status nest_solver_stream(nest_solver* s, void** stream);
 /* Device state: base pointer, row pitch (elements) and plane stride (elements). */
 nest_status nest_solver_state_ptr(nest_solver* s, void** dev, long long* pitch, long long* vstride);
 

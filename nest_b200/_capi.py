@@ -42,7 +42,7 @@ class SolverDesc(C.Structure):
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(
-            f"{LIB_PATH} is not built: run `python -m nest_b200.build` (needs nvcc for sm_100a)")
+            f"{LIB_PATH} is not built: run `python nest_b200/build.py` (needs nvcc for sm_100a)")
     return C.CDLL(str(LIB_PATH))
 
 
@@ -82,6 +82,11 @@ _SIGS = {
     "nest_solver_set_dt_sequence": (_i, [_vp, _dp, _i, _i]),
     "nest_solver_get_dts": (_i, [_vp, _dp, _i]),
     "nest_solver_state_ptr": (_i, [_vp, C.POINTER(_vp), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "nest_solver_set_exchange_sides": (_i, [_vp, _i, _i]),
+    "nest_solver_stage": (_i, [_vp, _i, _d, _d]),
+    "nest_solver_speed_slot": (_i, [_vp, C.POINTER(_vp)]),
+    "nest_solver_stage_ptr": (_i, [_vp, C.POINTER(_vp)]),
+    "nest_solver_stream": (_i, [_vp, C.POINTER(_vp)]),
     "nest_euler1d_run_noalloc": (_i, [_vp, _i, _i, _d, _d, _i, _d, _d, _ip, _dp, _vp]),
 }
 NOALLOC_MAX_CELLS = 65552

@@ -30,50 +30,44 @@ using namespace nestb::rt;
 
 namespace nestb {
 cudaError_t launch_1d_adjoint_stage(const double* U, const double* Lout, const double* Extra, double* Lin, int n,
-                                    int h, double lambda, double gamma, double alpha, double beta,
+                                    int h, const double* dtp, double dx, double gamma, double alpha, double beta,
                                     cudaStream_t st);
 }
 
 namespace {
 
-// Device operations the schedules need, for one solver form.
+// Device operations the schedules need, for one solver form.  Stage
+// launches take explicit loop parameters and parity (so a captured segment can
+// read its dts from device memory); adjoint steps read dt through a device
+// pointer.
 struct Stepper {
     virtual ~Stepper() = default;
-    virtual cudaError_t step(void* U, void* U1, double dt) = 0;          // U <- Heun step (U1 scratch)
-    virtual cudaError_t stage1(void* U, void* U1, double dt) = 0;        // U1 <- S(U)
-    virtual cudaError_t stage2(void* U, void* U1, double dt) = 0;        // U <- (U + S(U1)) / 2 after stage1
-    virtual cudaError_t adjoint_step(void* Un, void* U1, double dt, void* lam, void* lam_new, void* tmp) = 0;
+    // which = 1: U1 <- S(Un); which = 2: Uout <- (Un + S(U1)) / 2 after stage 1
+    virtual cudaError_t stage(int which, void* Un, void* U1, void* Uout, const LoopParams& lp, int p) = 0;
+    virtual cudaError_t adjoint_step(void* Un, void* U1, const double* dtp, void* lam, void* lam_new, void* tmp) = 0;
 };
+
+LoopParams fixed(double dt) {
+    LoopParams p{};
+    p.cfl = 1.0;
+    p.fixed_dt = dt;
+    return p;
+}
 
 struct Stepper1D : Stepper {
     nest_solver* s;
     StepCtrl* ctrl;
     explicit Stepper1D(nest_solver* s_, StepCtrl* c) : s(s_), ctrl(c) {}
-    LoopParams lp(double dt) const {
-        LoopParams p{};
-        p.cfl = 1.0;
-        p.fixed_dt = dt;
-        return p;
+    cudaError_t stage(int which, void* Un, void* U1, void* Uout, const LoopParams& lp, int p) override {
+        return launch_1d_step((double*)Un, (double*)U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp, ctrl, p,
+                              which, s->st, (double*)Uout);
     }
-    cudaError_t step(void* U, void* U1, double dt) override {
-        return launch_1d_step((double*)U, (double*)U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp(dt),
-                              ctrl, 0, 3, s->st);
-    }
-    cudaError_t stage1(void* U, void* U1, double dt) override {
-        return launch_1d_step((double*)U, (double*)U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp(dt),
-                              ctrl, 0, 1, s->st);
-    }
-    cudaError_t stage2(void* U, void* U1, double dt) override {
-        return launch_1d_step((double*)U, (double*)U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp(dt),
-                              ctrl, 0, 2, s->st);
-    }
-    cudaError_t adjoint_step(void* Un, void* U1, double dt, void* lam, void* lam_new, void* tmp) override {
-        double l = dt / s->d.dx;
+    cudaError_t adjoint_step(void* Un, void* U1, const double* dtp, void* lam, void* lam_new, void* tmp) override {
         cudaError_t e = launch_1d_adjoint_stage((const double*)U1, (const double*)lam, nullptr, (double*)tmp,
-                                                s->d.nx, s->h, l, s->d.gamma, 0.5, 0.0, s->st);
+                                                s->d.nx, s->h, dtp, s->d.dx, s->d.gamma, 0.5, 0.0, s->st);
         if (e != cudaSuccess) return e;
         return launch_1d_adjoint_stage((const double*)Un, (const double*)tmp, (const double*)lam,
-                                       (double*)lam_new, s->d.nx, s->h, l, s->d.gamma, 1.0, 0.5, s->st);
+                                       (double*)lam_new, s->d.nx, s->h, dtp, s->d.dx, s->d.gamma, 1.0, 0.5, s->st);
     }
 };
 
@@ -83,37 +77,27 @@ struct Stepper2D : Stepper {
     nest_solver* s;
     StepCtrl* ctrl;
     Stepper2D(nest_solver* s_, StepCtrl* c) : s(s_), ctrl(c) {}
-    LoopParams lp(double dt) const {
-        LoopParams p{};
-        p.cfl = 1.0;
-        p.fixed_dt = dt;
-        return p;
-    }
-    cudaError_t run(void* U, void* U1, double dt, int which) {
+    cudaError_t stage(int which, void* Un, void* U1, void* Uout, const LoopParams& lp, int p) override {
         if (s->d.precision == NEST_F64)
-            return launch_2d_step_f64((double*)U, (double*)U1, s->geo(), lp(dt), ctrl, nullptr, 0, s->tx, s->warps,
-                                      which, s->st);
-        return launch_2d_step_f32x2((float*)U, (float*)U1, s->geo(), lp(dt), ctrl, nullptr, 0, s->tx, s->warps,
-                                    (s->d.flags & NEST_FLAG_REPAIR) != 0, which, s->st);
+            return launch_2d_step_f64((double*)Un, (double*)U1, s->geo(), lp, ctrl, nullptr, p, s->tx, s->warps, which,
+                                      s->st, (double*)Uout);
+        return launch_2d_step_f32x2((float*)Un, (float*)U1, s->geo(), lp, ctrl, nullptr, p, s->tx, s->warps,
+                                    (s->d.flags & NEST_FLAG_REPAIR) != 0, which, s->st, (float*)Uout);
     }
-    cudaError_t step(void* U, void* U1, double dt) override { return run(U, U1, dt, 3); }
-    cudaError_t stage1(void* U, void* U1, double dt) override { return run(U, U1, dt, 1); }
-    cudaError_t stage2(void* U, void* U1, double dt) override { return run(U, U1, dt, 2); }
-    cudaError_t adjoint_step(void* Un, void* U1, double dt, void* lam, void* lam_new, void* tmp) override {
-        double lx = dt / s->d.dx, ly = dt / s->d.dy;
+    cudaError_t adjoint_step(void* Un, void* U1, const double* dtp, void* lam, void* lam_new, void* tmp) override {
         cudaError_t e;
         if (s->d.precision == NEST_F64) {
-            e = launch_2d_adjoint_stage_f64((const double*)U1, (const double*)lam, nullptr, (double*)tmp, s->geo(), lx,
-                                            ly, 0.5, 0.0, s->st);
+            e = launch_2d_adjoint_stage_f64((const double*)U1, (const double*)lam, nullptr, (double*)tmp, s->geo(), dtp,
+                                            0.5, 0.0, s->st);
             if (e == cudaSuccess)
                 e = launch_2d_adjoint_stage_f64((const double*)Un, (const double*)tmp, (const double*)lam,
-                                                (double*)lam_new, s->geo(), lx, ly, 1.0, 0.5, s->st);
+                                                (double*)lam_new, s->geo(), dtp, 1.0, 0.5, s->st);
         } else {
-            e = launch_2d_adjoint_stage_f32((const float*)U1, (const float*)lam, nullptr, (float*)tmp, s->geo(), lx,
-                                            ly, 0.5, 0.0, s->st);
+            e = launch_2d_adjoint_stage_f32((const float*)U1, (const float*)lam, nullptr, (float*)tmp, s->geo(), dtp,
+                                            0.5, 0.0, s->st);
             if (e == cudaSuccess)
                 e = launch_2d_adjoint_stage_f32((const float*)Un, (const float*)tmp, (const float*)lam,
-                                                (float*)lam_new, s->geo(), lx, ly, 1.0, 0.5, s->st);
+                                                (float*)lam_new, s->geo(), dtp, 1.0, 0.5, s->st);
         }
         return e;
     }
@@ -141,6 +125,10 @@ struct nest_adjoint {
     void* u1 = nullptr;
     void* lam[2] = {nullptr, nullptr};
     void* tmp = nullptr;
+    double* d_dts = nullptr;       // all dts (device), for the adjoint kernels of the binomial schedule
+    double* seg_dts = nullptr;     // dts of the current segment (device), uniform schedule
+    double* h_seg_dts = nullptr;   // pinned staging for seg_dts
+    std::map<int, cudaGraphExec_t> seg_graphs;  // uniform: one graph per segment length
     bool forward_done = false;
     double fwd_ms = 0.0, bwd_ms = 0.0;
     long long advanced = 0;        // forward steps run by the backward sweep (recompute)
@@ -164,7 +152,8 @@ nest_status copy_state_dev(nest_adjoint* a, void* dst, const void* src) {
 // Advance `work` (holding the state at step j0) by k steps.
 nest_status advance_work(nest_adjoint* a, int j0, int k) {
     for (int j = j0; j < j0 + k; ++j) {
-        cudaError_t e = a->stepper->step(a->work, a->u1, a->dts[j]);
+        cudaError_t e = a->stepper->stage(1, a->work, a->u1, nullptr, fixed(a->dts[j]), 0);
+        if (e == cudaSuccess) e = a->stepper->stage(2, a->work, a->u1, nullptr, fixed(a->dts[j]), 0);
         if (e != cudaSuccess) return cuda_fail(e, "recompute step");
         ++a->advanced;
     }
@@ -173,8 +162,8 @@ nest_status advance_work(nest_adjoint* a, int j0, int k) {
 
 // lambda <- adjoint of step j applied to lambda, given U^n of step j in `un`.
 nest_status reverse_one(nest_adjoint* a, void* un, int j, int& cur) {
-    cudaError_t e = a->stepper->stage1(un, a->u1, a->dts[j]);
-    if (e == cudaSuccess) e = a->stepper->adjoint_step(un, a->u1, a->dts[j], a->lam[cur], a->lam[cur ^ 1], a->tmp);
+    cudaError_t e = a->stepper->stage(1, un, a->u1, nullptr, fixed(a->dts[j]), 0);
+    if (e == cudaSuccess) e = a->stepper->adjoint_step(un, a->u1, a->d_dts + j, a->lam[cur], a->lam[cur ^ 1], a->tmp);
     if (e != cudaSuccess) return cuda_fail(e, "adjoint step");
     cur ^= 1;
     return NEST_OK;
@@ -208,6 +197,42 @@ nest_status reverse_binomial(nest_adjoint* a, int l, int r, int k, int free, int
     if ((st = reverse_binomial(a, m, r, k + 1, free - 1, cur)) != NEST_OK) return st;
     a->slot_pos[k + 1] = -1;
     return reverse_binomial(a, l, m, k, free, cur);
+}
+
+// Uniform schedule, one segment of L steps starting from seg_un[0]:
+// recompute (stage 1 into seg_u1[r], stage 2 out of place into seg_un[r+1],
+// dts read from seg_dts by step count) then reverse, lambda entering in
+// lam[0] and leaving in lam[0].  Captured once per L and replayed.
+nest_status segment_graph(nest_adjoint* a, int L, cudaGraphExec_t* out) {
+    auto it = a->seg_graphs.find(L);
+    if (it != a->seg_graphs.end()) { *out = it->second; return NEST_OK; }
+    cudaStream_t st = a->s->st;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaMemsetAsync(a->ctrl, 0, sizeof(StepCtrl), st);
+    LoopParams lp{};
+    lp.cfl = 1.0;
+    lp.dts_in = a->seg_dts;
+    lp.dts_cap = L;
+    for (int r = 0; r < L && e == cudaSuccess; ++r) {
+        e = a->stepper->stage(1, a->seg_un[r], a->seg_u1[r], nullptr, lp, r & 1);
+        if (e == cudaSuccess && r + 1 < L) e = a->stepper->stage(2, a->seg_un[r], a->seg_u1[r], a->seg_un[r + 1], lp, r & 1);
+    }
+    int cur = 0;
+    for (int r = L - 1; r >= 0 && e == cudaSuccess; --r, cur ^= 1)
+        e = a->stepper->adjoint_step(a->seg_un[r], a->seg_u1[r], a->seg_dts + r, a->lam[cur], a->lam[cur ^ 1], a->tmp);
+    if (e == cudaSuccess && cur == 1)
+        e = cudaMemcpyAsync(a->lam[0], a->lam[1], a->s->state_bytes(), cudaMemcpyDeviceToDevice, st);
+    cudaGraph_t g;
+    cudaError_t e2 = cudaStreamEndCapture(st, &g);
+    if (e != cudaSuccess) return cuda_fail(e, "segment capture");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+    cudaGraphExec_t ge;
+    cudaError_t e3 = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e3 != cudaSuccess) return cuda_fail(e3, "cudaGraphInstantiate");
+    a->seg_graphs[L] = ge;
+    *out = ge;
+    return NEST_OK;
 }
 
 // Steps at which the forward sweep stores snapshots: uniform multiples of K,
@@ -275,6 +300,11 @@ nest_status nest_adjoint_create(nest_solver* s, int nsteps, int policy, int para
     }
     for (void** p : {&a->work, &a->u1, &a->lam[0], &a->lam[1], &a->tmp})
         if ((st = adj_alloc(a, p)) != NEST_OK) return cleanup(st);
+    if ((e = cudaMalloc(&a->d_dts, sizeof(double) * nsteps)) != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(dts)"));
+    if ((e = cudaMalloc(&a->seg_dts, sizeof(double) * a->param)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "cudaMalloc(seg dts)"));
+    if ((e = cudaMallocHost(&a->h_seg_dts, sizeof(double) * a->param)) != cudaSuccess)
+        return cleanup(cuda_fail(e, "cudaMallocHost"));
     *out = a;
     return NEST_OK;
 }
@@ -287,6 +317,10 @@ nest_status nest_adjoint_destroy(nest_adjoint* a) {
     for (void* p : a->seg_un) cudaFree(p);
     for (void* p : a->seg_u1) cudaFree(p);
     for (void* p : {a->work, a->u1, a->lam[0], a->lam[1], a->tmp}) cudaFree(p);
+    for (auto& kv : a->seg_graphs) cudaGraphExecDestroy(kv.second);
+    cudaFree(a->d_dts);
+    cudaFree(a->seg_dts);
+    if (a->h_seg_dts) cudaFreeHost(a->h_seg_dts);
     cudaFree(a->ctrl);
     delete a;
     return NEST_OK;
@@ -326,6 +360,7 @@ nest_status nest_adjoint_forward(nest_adjoint* a, double cfl, const double* dts)
         if ((st = nest_solver_get_dts(s, a->dts.data(), a->nsteps)) != NEST_OK) return st;
     }
     if ((st = nest_solver_set_dt_sequence(s, nullptr, 0, 2)) != NEST_OK) return st;
+    CK(cudaMemcpy(a->d_dts, a->dts.data(), sizeof(double) * a->nsteps, cudaMemcpyHostToDevice));
     a->forward_done = true;
     return NEST_OK;
 }
@@ -347,21 +382,16 @@ nest_status nest_adjoint_backward(nest_adjoint* a, const void* lam_final, void* 
         int K = a->param;
         int nseg = (a->nsteps + K - 1) / K;
         for (int g = nseg - 1; g >= 0; --g) {
-            int j0 = g * K, j1 = std::min(a->nsteps, j0 + K);
-            if ((st = copy_state_dev(a, a->work, a->slots[g])) != NEST_OK) return st;
-            for (int j = j0; j < j1; ++j) {
-                if ((st = copy_state_dev(a, a->seg_un[j - j0], a->work)) != NEST_OK) return st;
-                cudaError_t e = a->stepper->stage1(a->work, a->seg_u1[j - j0], a->dts[j]);
-                if (e == cudaSuccess && j + 1 < j1) e = a->stepper->stage2(a->work, a->seg_u1[j - j0], a->dts[j]);
-                if (e != cudaSuccess) return cuda_fail(e, "segment recompute");
-                if (j + 1 < j1) ++a->advanced;
-            }
-            for (int j = j1 - 1; j >= j0; --j) {
-                cudaError_t e = a->stepper->adjoint_step(a->seg_un[j - j0], a->seg_u1[j - j0], a->dts[j],
-                                                         a->lam[cur], a->lam[cur ^ 1], a->tmp);
-                if (e != cudaSuccess) return cuda_fail(e, "adjoint step");
-                cur ^= 1;
-            }
+            int j0 = g * K, L = std::min(a->nsteps, j0 + K) - j0;
+            cudaGraphExec_t ge;
+            if ((st = segment_graph(a, L, &ge)) != NEST_OK) return st;
+            for (int r = 0; r < L; ++r) a->h_seg_dts[r] = a->dts[j0 + r];
+            CK(cudaMemcpyAsync(a->seg_dts, a->h_seg_dts, sizeof(double) * L, cudaMemcpyHostToDevice, s->st));
+            if ((st = copy_state_dev(a, a->seg_un[0], a->slots[g])) != NEST_OK) return st;
+            CK(cudaGraphLaunch(ge, s->st));
+            // the staging buffer is reused by the next segment
+            CK(cudaStreamSynchronize(s->st));
+            a->advanced += L - 1;
         }
     } else {
         if ((st = reverse_binomial(a, 0, a->nsteps, 0, a->param - 1, cur)) != NEST_OK) return st;

@@ -4,7 +4,7 @@
 //   W_c   = prim(U_c)                          (euler1d.hpp:69-84, p clamped at 0)
 //   s_c   = minmod(W_c - W_{c-1}, W_{c+1} - W_c)
 //   F_f   = HLLE(W_a + s_a/2, W_b - s_b/2)     (face f between cells a = b-1 and b)
-//   U'_i  = U_i - lambda (F_{i+1/2} - F_{i-1/2}),  lambda = dt/dx
+//   U'_i  = U_i - lambda (F_{i+1/2} - F_{i-1/2}),  lambda = dt/dx (dt read from device memory)
 // Adjoint (dt frozen), for a given adjoint Ubar' of the stage output:
 //   Fbar_f   = lambda (Ubar'_b - Ubar'_a)
 //   WLbar_f, WRbar_f = HLLE Jacobians^T Fbar_f   (branch of the forward: S_L >= 0,
@@ -85,13 +85,20 @@ __device__ void hlle1d_adj(double gamma, double gm1, St3 L, St3 R, const double 
     side(R, ER, cR, fRb, uRb, uRb_, cRb, wr);
 }
 
-__device__ __forceinline__ int wrap(int c, int n) { return c < 0 ? c + n : (c >= n ? c - n : c); }
+// Periodic index.  Tile halo cells past the domain (read by threads that
+// return early) can lie more than one period away on small domains.
+__device__ __forceinline__ int wrap(int c, int n) {
+    int r = c % n;
+    return r < 0 ? r + n : r;
+}
 
 // Lin = alpha * adj(U, Lout) + beta * Extra (Extra may be null).  U, Lout,
 // Extra, Lin: SoA [3][n + 2h], interior at offset h; periodic.
 __global__ void __launch_bounds__(TA)
 k1d_adjoint_stage(const double* __restrict__ U, const double* __restrict__ Lout, const double* __restrict__ Extra,
-                  double* __restrict__ Lin, int n, int h, double lambda, double gamma, double alpha, double beta) {
+                  double* __restrict__ Lin, int n, int h, const double* dtp, double dx, double gamma, double alpha,
+                  double beta) {
+    const double lambda = *dtp / dx;
     __shared__ double W[3][TA + 6];     // cells c0-3 .. c0+TA+2
     __shared__ double Lo[3][TA + 4];    // cells c0-2 .. c0+TA+1 (alpha applied)
     __shared__ double S[3][TA + 4];     // slopes of cells c0-2 .. c0+TA+1
@@ -175,10 +182,10 @@ k1d_adjoint_stage(const double* __restrict__ U, const double* __restrict__ Lout,
 }  // namespace
 
 cudaError_t launch_1d_adjoint_stage(const double* U, const double* Lout, const double* Extra, double* Lin, int n,
-                                    int h, double lambda, double gamma, double alpha, double beta,
+                                    int h, const double* dtp, double dx, double gamma, double alpha, double beta,
                                     cudaStream_t st) {
     int blocks = (n + TA - 1) / TA;
-    k1d_adjoint_stage<<<blocks, TA, 0, st>>>(U, Lout, Extra, Lin, n, h, lambda, gamma, alpha, beta);
+    k1d_adjoint_stage<<<blocks, TA, 0, st>>>(U, Lout, Extra, Lin, n, h, dtp, dx, gamma, alpha, beta);
     return cudaGetLastError();
 }
 

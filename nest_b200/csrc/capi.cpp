@@ -535,6 +535,57 @@ nest_status nest_solver_get_dts(nest_solver* s, double* dts, int n) {
     return NEST_OK;
 }
 
+nest_status nest_solver_set_exchange_sides(nest_solver* s, int xlo, int xhi) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (s->d.dim != 2) return fail(NEST_ERR_UNSUPPORTED, "halo-exchange sides apply to 2D solvers");
+    if (s->d.flags & NEST_FLAG_SPLIT_COMPAT) return fail(NEST_ERR_UNSUPPORTED, "sharding runs the RK2 scheme");
+    CK(cudaStreamSynchronize(s->st));
+    s->xlo_ex = xlo ? 1 : 0;
+    s->xhi_ex = xhi ? 1 : 0;
+    s->prepared = false;
+    drop_graphs(s);
+    return NEST_OK;
+}
+
+nest_status nest_solver_stage(nest_solver* s, int which, double cfl, double t_final) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (which != 1 && which != 2) return fail(NEST_ERR_INVALID, "stage must be 1 or 2");
+    if (!(cfl > 0.0)) return fail(NEST_ERR_INVALID, "cfl must be positive");
+    if (s->resident()) return fail(NEST_ERR_UNSUPPORTED, "single stages use the tiled path (NEST_FLAG_NO_RESIDENT)");
+    if (!s->prepared && (r = prepare(s)) != NEST_OK) return r;
+    LoopParams lp = base_params(s);
+    lp.cfl = cfl;
+    lp.t_final = t_final > 0.0 ? t_final : 0.0;
+    cudaError_t e = enqueue_step(s, lp, s->parity, which);
+    if (e != cudaSuccess) return cuda_fail(e, "stage launch");
+    if (which == 2) s->parity ^= 1;
+    return NEST_OK;
+}
+
+nest_status nest_solver_speed_slot(nest_solver* s, void** dev) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (!s->prepared && (r = prepare(s)) != NEST_OK) return r;
+    if (dev) *dev = &s->ctrl->maxs[s->parity][0];
+    return NEST_OK;
+}
+
+nest_status nest_solver_stage_ptr(nest_solver* s, void** dev) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (dev) *dev = s->U1;
+    return NEST_OK;
+}
+
+nest_status nest_solver_stream(nest_solver* s, void** stream) {
+    nest_status r = check(s);
+    if (r != NEST_OK) return r;
+    if (stream) *stream = (void*)s->st;
+    return NEST_OK;
+}
+
 nest_status nest_solver_state_ptr(nest_solver* s, void** dev, long long* pitch, long long* vstride) {
     nest_status r = check(s);
     if (r != NEST_OK) return r;
@@ -765,6 +816,7 @@ nest_status nest_batch_create(const nest_batch_desc* d, nest_batch** out) {
         g.dx = d->dx ? d->dx[p] : 1.0 / g.nx;
         g.dy = d->dy ? d->dy[p] : 1.0 / g.ny;
         g.gamma = d->gamma;
+        g.xlo_ex = 0; g.xhi_ex = 0;
         b->probs[p].g = g;
         b->probs[p].off = off;
         off += 4 * g.vstride;

@@ -324,10 +324,10 @@ cudaError_t launch_1d_prepare(double* U, int n, int h, double gamma, int bc, Ste
 }
 
 cudaError_t launch_1d_step(double* U, double* U1, int n, int h, double dx, double gamma, int bc,
-                           const LoopParams& lp, StepCtrl* ctrl, int p, int which, cudaStream_t st) {
+                           const LoopParams& lp, StepCtrl* ctrl, int p, int which, cudaStream_t st, double* Uout) {
     int blocks = (n + T1 - 1) / T1;
     if (which & 1) k1d_stage<1><<<blocks, T1, 0, st>>>(U, nullptr, U1, n, h, dx, gamma, bc, lp, ctrl, p);
-    if (which & 2) k1d_stage<2><<<blocks, T1, 0, st>>>(U1, U, U, n, h, dx, gamma, bc, lp, ctrl, p);
+    if (which & 2) k1d_stage<2><<<blocks, T1, 0, st>>>(U1, U, Uout ? Uout : U, n, h, dx, gamma, bc, lp, ctrl, p);
     return cudaGetLastError();
 }
 

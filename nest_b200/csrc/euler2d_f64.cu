@@ -23,14 +23,19 @@ cudaError_t launch_2d_prepare_f64(double* U, const Geo2D& g, StepCtrl* ctrl, int
 
 cudaError_t launch_2d_step_f64(double* U, double* U1, const Geo2D& g, const LoopParams& lp,
                                StepCtrl* ctrl, double* partials, int p, int tx, int warps,
-                               int which, cudaStream_t st) {
+                               int which, cudaStream_t st, double* Uout) {
     int nstrips = (g.ny + STRIP - 1) / STRIP;
     dim3 b(32, warps), gr((nstrips + warps - 1) / warps, (g.nx + tx - 1) / tx);
     StageArgs<double> a1{U, nullptr, U1, g, lp, ctrl, nullptr, p, tx};
     if (which & 1) k2d_f64<1><<<gr, b, 0, st>>>(a1);
-    StageArgs<double> a2{U1, U, U, g, lp, ctrl, partials, p, tx};
+    StageArgs<double> a2{U1, U, Uout ? Uout : U, g, lp, ctrl, partials, p, tx};
     if (which & 2) k2d_f64<2><<<gr, b, 0, st>>>(a2);
     return cudaGetLastError();
+}
+
+template <int STAGE>
+__device__ __noinline__ void f64_body_call(const StageArgs<double>& a, int strip, int tile_row) {
+    stage2d_body<double, STAGE, false>(a, strip, tile_row);
 }
 
 // Persistent batched FP64 stage (bit-exact per problem).
@@ -43,7 +48,7 @@ __global__ void __launch_bounds__(256) kbatch_f64(BatchArgs<double> b) {
         StageArgs<double> a{STAGE == 1 ? b.U + P.off : b.U1 + P.off, STAGE == 2 ? b.U + P.off : nullptr,
                             STAGE == 1 ? b.U1 + P.off : b.U + P.off, P.g, b.lp, b.ctrls + w.x,
                             (STAGE == 2 && b.partials) ? b.partials + 4ll * P.item0 : nullptr, b.p, b.tx};
-        stage2d_body<double, STAGE, false>(a, w.y, w.z);
+        f64_body_call<STAGE>(a, w.y, w.z);
     }
 }
 

@@ -56,6 +56,7 @@ struct Geo2D {
     long long vstride;    // elements per variable plane
     int bcx, bcy;         // boundary condition along x (rows) and y (columns)
     double dx, dy, gamma;
+    int xlo_ex, xhi_ex;   // 1: that x side's ghost rows are filled by a halo exchange (sharded domain)
     __device__ __forceinline__ long long at(int i, int j) const {
         return (long long)(i + 2) * pitch + (j + 2);
     }
@@ -181,11 +182,11 @@ __device__ __forceinline__ void store_ghosts(T* Uo, const Geo2D& g, int k, int i
         if (j == g.ny - 1) { p[g.at(i, g.ny)] = v; p[g.at(i, g.ny + 1)] = v; }
     }
     if (g.bcx == BC_PERIODIC) {
-        if (i < 2) p[g.at(i + g.nx, j)] = v;
-        if (i >= g.nx - 2) p[g.at(i - g.nx, j)] = v;
+        if (i < 2 && !g.xhi_ex) p[g.at(i + g.nx, j)] = v;
+        if (i >= g.nx - 2 && !g.xlo_ex) p[g.at(i - g.nx, j)] = v;
     } else {
-        if (i == 0) { p[g.at(-1, j)] = v; p[g.at(-2, j)] = v; }
-        if (i == g.nx - 1) { p[g.at(g.nx, j)] = v; p[g.at(g.nx + 1, j)] = v; }
+        if (i == 0 && !g.xlo_ex) { p[g.at(-1, j)] = v; p[g.at(-2, j)] = v; }
+        if (i == g.nx - 1 && !g.xhi_ex) { p[g.at(g.nx, j)] = v; p[g.at(g.nx + 1, j)] = v; }
     }
 }
 
@@ -421,6 +422,7 @@ __device__ __forceinline__ void prepare2d_body(T* U, const Geo2D& g, StepCtrl* c
     j -= 2; i -= 2;
     double smx = 0.0, smy = 0.0;
     bool in = (j >= -2 && j < g.ny + 2 && i >= -2 && i < g.nx + 2);
+    if ((i < 0 && g.xlo_ex) || (i >= g.nx && g.xhi_ex)) in = false;  // filled by the halo exchange
     if (in) {
         // source cell: wrap (periodic) or clamp (outflow) each axis
         int si = i, sj = j;

@@ -21,14 +21,17 @@ cudaError_t launch_1d_resident(double* U, int n, int h, double dx, double gamma,
                                const LoopParams& lp, StepCtrl* ctrl, int p, cudaStream_t st);
 cudaError_t launch_1d_prepare(double* U, int n, int h, double gamma, int bc, StepCtrl* ctrl, int p,
                               cudaStream_t st);
+// Stage 1 reads U and writes U1; stage 2 reads U1 and U and writes Uout
+// (null: U, in place).
 cudaError_t launch_1d_step(double* U, double* U1, int n, int h, double dx, double gamma, int bc,
-                           const LoopParams& lp, StepCtrl* ctrl, int p, int which, cudaStream_t st);
+                           const LoopParams& lp, StepCtrl* ctrl, int p, int which, cudaStream_t st,
+                           double* Uout = nullptr);
 
 // 2D unsplit scheme.  `which`: 1 = stage 1, 2 = stage 2, 3 = both.
 cudaError_t launch_2d_prepare_f64(double* U, const Geo2D& g, StepCtrl* ctrl, int p, cudaStream_t st);
 cudaError_t launch_2d_step_f64(double* U, double* U1, const Geo2D& g, const LoopParams& lp,
                                StepCtrl* ctrl, double* partials, int p, int tx, int warps,
-                               int which, cudaStream_t st);
+                               int which, cudaStream_t st, double* Uout = nullptr);
 cudaError_t launch_2d_prepare_f32(float* U, const Geo2D& g, StepCtrl* ctrl, int p, cudaStream_t st);
 cudaError_t launch_2d_step_f32(float* U, float* U1, const Geo2D& g, const LoopParams& lp,
                                StepCtrl* ctrl, double* partials, int p, int tx, int warps,
@@ -37,18 +40,19 @@ cudaError_t launch_2d_step_f32(float* U, float* U1, const Geo2D& g, const LoopPa
 // columns per warp).
 cudaError_t launch_2d_step_f32x2(float* U, float* U1, const Geo2D& g, const LoopParams& lp, StepCtrl* ctrl,
                                  double* partials, int p, int tx, int warps, bool repair, int which,
-                                 cudaStream_t st);
+                                 cudaStream_t st, float* Uout = nullptr);
 
 // nest's split 2D scheme (x-sweep = stage 1, y-sweep = stage 2), FP64.
 cudaError_t launch_2d_compat_step(double* U, double* U1, const Geo2D& g, const LoopParams& lp, StepCtrl* ctrl, int p,
                                   int which, cudaStream_t st);
 
 // Adjoint of one 2D stage: Lin = alpha * adj(U, Lout) + beta * Extra (periodic).
+// dt is read on the device from *dtp (lx = dt/dx, ly = dt/dy).
 cudaError_t launch_2d_adjoint_stage_f64(const double* U, const double* Lout, const double* Extra, double* Lin,
-                                        const Geo2D& g, double lx, double ly, double alpha, double beta,
+                                        const Geo2D& g, const double* dtp, double alpha, double beta,
                                         cudaStream_t st);
 cudaError_t launch_2d_adjoint_stage_f32(const float* U, const float* Lout, const float* Extra, float* Lin,
-                                        const Geo2D& g, double lx, double ly, double alpha, double beta,
+                                        const Geo2D& g, const double* dtp, double alpha, double beta,
                                         cudaStream_t st);
 
 // Batched persistent stages (one launch per stage over the work list).

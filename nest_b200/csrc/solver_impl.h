@@ -70,6 +70,7 @@ struct nest_solver {
     int parity = 0;
     bool prepared = false;
     int tx = 64, warps = 4;
+    int xlo_ex = 0, xhi_ex = 0;    // sharded domain: x sides filled by a halo exchange
     std::map<nestb::rt::GraphKey, cudaGraphExec_t> graphs;
 
     bool resident() const {
@@ -80,6 +81,7 @@ struct nest_solver {
         nestb::Geo2D g;
         g.nx = d.nx; g.ny = d.ny; g.pitch = pitch; g.vstride = vstride;
         g.bcx = d.bc_x; g.bcy = d.bc_y; g.dx = d.dx; g.dy = d.dy; g.gamma = d.gamma;
+        g.xlo_ex = xlo_ex; g.xhi_ex = xhi_ex;
         return g;
     }
     size_t state_bytes() const { return esize * (size_t)nvars * (size_t)vstride; }

@@ -38,10 +38,12 @@ def prim_to_cons_2d(rho, u, v, p, gamma: float = GAMMA) -> np.ndarray:
     return U
 
 
-def riemann_2d(nx: int, ny: int, gamma: float = GAMMA) -> np.ndarray:
+def riemann_2d(nx: int, ny: int, gamma: float = GAMMA, rows: tuple[int, int] | None = None) -> np.ndarray:
     """Diagonal 2D Riemann problem on [0,1]^2: (1, 0, 0, 1) where x + y < 1 at
-    cell centres, else (0.125, 0, 0, 0.1)."""
-    x = (np.arange(-2, nx + 2) + 0.5) / nx
+    cell centres, else (0.125, 0, 0, 0.1).  rows = (x0, n) returns only the
+    extended rows of that x-slab ([4][n+4][ny+4])."""
+    x0, n = rows if rows is not None else (0, nx)
+    x = (np.arange(x0 - 2, x0 + n + 2) + 0.5) / nx
     y = (np.arange(-2, ny + 2) + 0.5) / ny
     X, Y = np.meshgrid(x, y, indexing="ij")
     left = (X + Y) < 1.0
@@ -90,6 +92,33 @@ def fourier_fields_1d(n: int, seed: int, modes: int = 16):
         out.append(f / np.abs(f).max())
     f, g, h = out
     return 1.0 + 0.5 * f, 0.3 * g, 1.0 + 0.5 * h
+
+
+def fourier_fields_2d(nx: int, ny: int, seed: int, modes: int = 4, gamma: float = GAMMA) -> np.ndarray:
+    """Smooth periodic conserved state [4][nx+4][ny+4] on [0,1)^2 (ghosts zero):
+    rho, u, v, p each a random sum of modes (kx, ky) in [0, modes]^2 of
+    a cos(2 pi (kx x + ky y) + phi), a ~ N(0, 1), phi ~ U(0, 2 pi) (numpy PCG64,
+    `seed`), scaled to rho = 1 + 0.4 f, u = 0.3 g, v = 0.3 h, p = 1 + 0.4 q with
+    max|f| = max|g| = max|h| = max|q| = 1.  No region is uniform, so no limiter
+    slope sits at the minmod(0, 0) corner."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(nx) + 0.5) / nx
+    y = (np.arange(ny) + 0.5) / ny
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    out = []
+    for _ in range(4):
+        f = np.zeros((nx, ny))
+        for kx in range(modes + 1):
+            for ky in range(modes + 1):
+                if kx == 0 and ky == 0:
+                    continue
+                a, phi = rng.standard_normal(), rng.uniform(0.0, 2.0 * np.pi)
+                f += a * np.cos(2 * np.pi * (kx * X + ky * Y) + phi)
+        out.append(f / np.abs(f).max())
+    f, g, h, q = out
+    U = np.zeros((4, nx + 4, ny + 4))
+    U[:, 2:-2, 2:-2] = prim_to_cons_2d(1.0 + 0.4 * f, 0.3 * g, 0.3 * h, 1.0 + 0.4 * q, gamma)
+    return U
 
 
 def prim_to_cons_1d(rho, u, p, gamma: float = GAMMA, h: int = 2) -> np.ndarray:

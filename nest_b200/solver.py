@@ -193,3 +193,29 @@ class Solver:
         p, pitch, vs = C.c_void_p(), C.c_longlong(), C.c_longlong()
         check(lib.nest_solver_state_ptr(self._h, C.byref(p), C.byref(pitch), C.byref(vs)), "nest_solver_state_ptr")
         return p.value, pitch.value, vs.value
+
+    # -- stage-level driving (sharded domains) --------------------------------
+    def set_exchange_sides(self, xlo: bool, xhi: bool):
+        """Mark x sides whose ghost rows a halo exchange fills (the kernels
+        leave them alone)."""
+        check(lib.nest_solver_set_exchange_sides(self._h, int(xlo), int(xhi)), "nest_solver_set_exchange_sides")
+
+    def stage(self, which: int, cfl: float, t_final: float = 0.0):
+        """Enqueue stage 1 (U -> U1, derives dt from the speed slot) or stage 2
+        (U1 -> U, reduces the next step's wave speeds) of the current step."""
+        check(lib.nest_solver_stage(self._h, which, cfl, t_final), "nest_solver_stage")
+
+    def speed_slot_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib.nest_solver_speed_slot(self._h, C.byref(p)), "nest_solver_speed_slot")
+        return p.value
+
+    def stage_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib.nest_solver_stage_ptr(self._h, C.byref(p)), "nest_solver_stage_ptr")
+        return p.value
+
+    def stream_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib.nest_solver_stream(self._h, C.byref(p)), "nest_solver_stream")
+        return p.value or 0

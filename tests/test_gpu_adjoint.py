@@ -135,10 +135,10 @@ def test_autograd_rollout(gpu):
     assert abs(ad - fd) <= 1e-6 * abs(fd), (ad, fd)
 
 
-def adjoint2d_case(gpu, nx, ny, nsteps, prec, seed=3, policy=0, param=8):
+def adjoint2d_case(gpu, nx, ny, nsteps, prec, seed=3, policy=0, param=8, smooth=False):
     from nest_b200.adjoint import Adjoint
-    from nest_b200.problems import kelvin_helmholtz
-    U0 = kelvin_helmholtz(nx, ny, seed=seed)
+    from nest_b200.problems import fourier_fields_2d, kelvin_helmholtz
+    U0 = fourier_fields_2d(nx, ny, seed) if smooth else kelvin_helmholtz(nx, ny, seed=seed)
     dt = np.float64 if prec == gpu.F64 else np.float32
     s = gpu.Solver(2, nx, ny, bc=gpu.BC_PERIODIC, precision=prec)
     s.upload(U0.astype(dt))
@@ -179,8 +179,13 @@ def ke_v_loss_and_lambda(U, nx, ny):
 
 
 def test_adjoint2d_finite_differences_fp64(gpu):
+    """Central differences against the adjoint on a smooth state.  The KH
+    state has exactly uniform bands where the limiter sits at minmod(0, 0):
+    there the scheme is only piecewise linear and a difference quotient
+    measures a one-sided derivative the subgradient does not (the exact
+    tangent test covers KH)."""
     nx, ny, nsteps = 48, 40, 30
-    U0, s, adj = adjoint2d_case(gpu, nx, ny, nsteps, gpu.F64, seed=4)
+    U0, s, adj = adjoint2d_case(gpu, nx, ny, nsteps, gpu.F64, seed=4, smooth=True)
     dts = adj.dts()
     L0, lamT = ke_v_loss_and_lambda(s.download(), nx, ny)
     lam0 = adj.backward(lamT)
