@@ -62,6 +62,10 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=500)
     ap.add_argument("--adjoint-n", type=int, default=65536)
     ap.add_argument("--adjoint-steps", type=int, default=2000)
+    ap.add_argument("--fd-directions", type=int, default=32)
+    ap.add_argument("--adjoint2d-n", type=int, default=2048)
+    ap.add_argument("--adjoint2d-steps", type=int, default=4000)
+    ap.add_argument("--no-adjoint2d", action="store_true")
     return ap.parse_args()
 
 
@@ -101,6 +105,16 @@ def barrier(ws):
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def allsum(ws, x: float) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
 
 
 def allmax(ws, x: float) -> float:
@@ -307,6 +321,8 @@ def run_ours(args, ws, rank, local):
     time.sleep(0.3)
     forms = [f.strip() for f in args.forms.split(",") if f.strip()]
     launches = 0
+    rho_final = {}
+    from nest_b200.exact_riemann import l1_rho_diagonal
     for form in forms:
         if ws > 1 or args.slab_path:
             r = run_slabs(args, ws, rank, form, cfl, st)
@@ -362,6 +378,7 @@ def run_ours(args, ws, rank, local):
         e1.record(st)
         e1.synchronize()
         graph_ms = e0.elapsed_time(e1) / args.steps
+        rho_final[form] = s.download()[0, 2:-2, 2:-2].astype(np.float64)
         ab = alg_bytes_per_cell(form)
         m1, m2 = float(np.mean(k1)), float(np.mean(k2))
         dom, dom_ms = ("stage2", m2) if m2 >= m1 else ("stage1", m1)
@@ -378,12 +395,17 @@ def run_ours(args, ws, rank, local):
                          "alg_bytes_per_launch": ab[dom] * cells,
                          "traffic": (tr or {}).get(dom)},
             "window": (t0, t1),
+            "l1_rho_vs_exact": l1_rho_diagonal(rho_final[form], tsim, margin=0.05),
         }
         if not args.no_e2e:
             results[form]["e2e"] = e2e_run(s, U, args.steps, cfl, st, cells, ws)
         s.close()
         del s
     clocks.stop()
+    if "f32" in rho_final and "f64" in rho_final:
+        d = np.abs(rho_final["f32"] - rho_final["f64"])
+        results["f32"]["rho_vs_f64"] = {"max_abs": float(d.max()), "l1": float(d.mean())}
+    rho_final.clear()
     head = forms[0]
     r = results[head]
     clk = clocks.summary(min(x["window"][0] for x in results.values()), max(x["window"][1] for x in results.values()))
@@ -409,6 +431,9 @@ def run_ours(args, ws, rank, local):
     if not args.no_extras:
         out["batched_kh"] = bench_batch(args, ws)
         out["adjoint_1d"] = bench_adjoint(args)
+        out["sod_1d"] = bench_sod1d()
+        if not args.no_adjoint2d:
+            out["adjoint_2d_kh"] = bench_adjoint2d(args)
         out["gpu_launches_extras"] = out["batched_kh"]["launches"] + out["adjoint_1d"]["launches"]
     if ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(n, args.cpu_seconds)
@@ -424,10 +449,13 @@ def bench_batch(args, ws):
     import nest_b200 as nb
     from nest_b200.problems import kelvin_helmholtz, kh_sizes
     nx, ny = kh_sizes(args.batch_count, seed=0)
+    rank = int(os.environ.get("RANK", "0"))
+    ids = np.arange(rank, len(nx), ws)          # problems are independent: rank r takes r, r+ws, ...
+    nx, ny = nx[ids], ny[ids]
     st = torch.cuda.Stream()
     from nest_b200.tuning import best_batch_tiling
     b = nb.Batch(nx, ny, precision=nb.F32, flags=nb.FLAG_TOTALS | nb.FLAG_REPAIR, stream=st.cuda_stream)
-    ics = [kelvin_helmholtz(int(nx[p]), int(ny[p]), seed=1 + p).astype(np.float32) for p in range(len(nx))]
+    ics = [kelvin_helmholtz(int(nx[p]), int(ny[p]), seed=1 + int(ids[p])).astype(np.float32) for p in range(len(nx))]
     for p, U in enumerate(ics):
         b.upload(p, U)
     tiling = best_batch_tiling(b, nx, ny)  # may advance the states: re-upload below
@@ -446,14 +474,16 @@ def bench_batch(args, ws):
     e1.record(st)
     e1.synchronize()
     ms = allmax(ws, e0.elapsed_time(e1))
+    cells = allsum(ws, cells)
     times, steps = b.times()
     tot = b.totals()
     drift = np.abs(tot - t0).max(axis=0) / np.maximum(np.abs(t0).max(axis=0), 1e-300)
-    value = ws * cells * 2 * args.batch_steps / (ms * 1e-3)
+    value = cells * 2 * args.batch_steps / (ms * 1e-3)
     b.close()
-    return {"value": value, "unit": UNIT, "problems": int(len(nx)), "cells": int(cells), "steps": args.batch_steps,
+    return {"value": value, "unit": UNIT, "problems": args.batch_count, "problems_per_rank": int(len(nx)),
+            "sharding": f"by problem over {ws} rank(s), no collective", "cells": int(cells), "steps": args.batch_steps,
             "ms_total": ms, "ms_per_step": ms / args.batch_steps, "work_items": items, "persistent_blocks": blocks,
-            "hbm_gbs_equiv": value / ws * 40 / 1e9, "sim_time_range": [float(times.min()), float(times.max())],
+            "hbm_gbs_equiv_per_gpu": value / ws * 40 / 1e9, "sim_time_range": [float(times.min()), float(times.max())],
             "fp64_totals_rel_drift": {"mass": float(drift[0]), "energy": float(drift[3])},
             "tiling": {"rows_per_item": tiling[0], "warps_per_block": tiling[1], "blocks_per_sm": tiling[2]},
             "launches": 2 * args.batch_steps, "dtype": "f32 (FP64 totals, time, repair)"}
@@ -480,13 +510,126 @@ def bench_adjoint(args):
     UT = s.download()
     lam = np.zeros_like(UT)
     lam[0, 2:-2] = (UT[0, 2:-2] - tgt) / n
-    a.backward(lam)
+    lam0 = a.backward(lam)
     st = a.stats()
     fwd, bwd = st["forward_ms"], st["backward_ms"]
-    return {"n": n, "steps": K, "checkpoint_every": 64, "forward_ms": fwd, "backward_ms": bwd,
+    fd = fd_check_1d(lambda: nb.Solver(1, n, bc=nb.BC_PERIODIC, flags=nb.FLAG_NO_RESIDENT), U0, tgt, n, K,
+                     a.dts(), lam0, ndir=args.fd_directions) if args.fd_directions > 0 else None
+    return {"n": n, "steps": K, "checkpoint_every": 64, "forward_ms": fwd, "backward_ms": bwd, "fd_check": fd,
             "adjoint_over_forward": bwd / fwd, "gradient_over_forward": (fwd + bwd) / fwd,
             "recomputed_steps": st["recomputed_steps"], "checkpoint_mb": st["checkpoint_bytes"] / 1e6,
             "launches": 2 * K + 2 * K + 3 * K, "dtype": "f64"}
+
+
+def bench_sod1d(reps: int = 20):
+    """1D Sod: N = 1024, outflow, CFL 0.4 to t = 0.2, FP64 (one resident CTA
+    runs the whole loop).  Device time of run_to from the initial state;
+    L1(rho) against the exact solution."""
+    import torch
+    import nest_b200 as nb
+    from nest_b200.exact_riemann import l1_rho_1d
+    from nest_b200.problems import sod_1d
+    n = 1024
+    s = nb.Solver(1, n, bc=nb.BC_OUTFLOW)
+    U0 = sod_1d(n)
+    ext = torch.cuda.ExternalStream(s.stream_ptr())
+    s.upload(U0)
+    s.run_to(0.2, 0.4)
+    ms = []
+    for _ in range(reps):
+        s.upload(U0)
+        s.reset_time()
+        s.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        steps = s.run_to(0.2, 0.4)
+        e1.record(ext)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t, _ = s.time()
+    rho = s.download()[0, 2:-2]
+    m = float(np.median(ms))
+    s.close()
+    return {"n": n, "bc": "outflow", "cfl": 0.4, "t_final": t, "steps": steps, "ms": m,
+            "value": n * steps * 2 / (m * 1e-3), "unit": UNIT, "l1_rho_vs_exact": l1_rho_1d(rho, t),
+            "launches": 1, "dtype": "f64", "kernel": "k1d_resident (whole run in one CTA's shared memory)"}
+
+
+def ke_v(U, nx, ny):
+    """L = integral of 1/2 rho v^2 dA over the interior and dL/dU (extended layout)."""
+    r, mv = U[0, 2:-2, 2:-2].astype(np.float64), U[2, 2:-2, 2:-2].astype(np.float64)
+    v = mv / r
+    dA = 1.0 / (nx * ny)
+    lam = np.zeros(U.shape)
+    lam[0, 2:-2, 2:-2] = -0.5 * v * v * dA
+    lam[2, 2:-2, 2:-2] = v * dA
+    return 0.5 * float(np.sum(r * v * v)) * dA, lam
+
+
+def bench_adjoint2d(args):
+    """Kelvin-Helmholtz on one periodic n x n grid (seed 1), K steps at CFL
+    0.4, loss = integral of 1/2 rho v^2 dA at the end, binomial
+    checkpointing with as many snapshots as fit in 40 GB; gradient with
+    respect to the initial v field (rho, u, p held), FP64 and FP32; the FP32
+    gradient is compared with the FP64 one."""
+    import nest_b200 as nb
+    from nest_b200.adjoint import BINOMIAL, Adjoint
+    from nest_b200.problems import kelvin_helmholtz
+    n, K = args.adjoint2d_n, args.adjoint2d_steps
+    U0 = kelvin_helmholtz(n, n, seed=1)
+    out, grads = {}, {}
+    for form, prec, dt in (("f64", nb.F64, np.float64), ("f32", nb.F32, np.float32)):
+        s = nb.Solver(2, n, n, bc=nb.BC_PERIODIC, precision=prec)
+        _, pitch, vs = s.state_ptr()
+        slots = int(min(K, 40e9 // (4 * vs * np.dtype(dt).itemsize)))
+        s.upload(U0.astype(dt))
+        a = Adjoint(s, K, BINOMIAL, slots)
+        a.forward(0.4)
+        UT = s.download()
+        L, lam = ke_v(UT, n, n)
+        lam0 = a.backward(lam.astype(dt)).astype(np.float64)
+        st = a.stats()
+        r0, ru0, rv0 = U0[0, 2:-2, 2:-2], U0[1, 2:-2, 2:-2], U0[2, 2:-2, 2:-2]
+        # dL/dv0 with rho, u, p held: d(rho v)/dv = rho, dE/dv = rho v
+        grads[form] = lam0[2, 2:-2, 2:-2] * r0 + lam0[3, 2:-2, 2:-2] * rv0
+        out[form] = {"forward_ms": st["forward_ms"], "backward_ms": st["backward_ms"],
+                     "adjoint_over_forward": st["backward_ms"] / st["forward_ms"],
+                     "recomputed_steps": st["recomputed_steps"], "snapshots": slots,
+                     "checkpoint_gb": st["checkpoint_bytes"] / 1e9, "loss": L}
+        a.close()
+        s.close()
+    g64, g32 = grads["f64"], grads["f32"]
+    out["f32_vs_f64_grad_rel_l2"] = float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))
+    out.update({"n": n, "steps": K, "policy": "binomial (snapshots fitting 40 GB)",
+                "loss": "integral of 1/2 rho v^2 dA at t_end", "gradient": "d loss / d v(t=0)",
+                "launches": None})
+    return out
+
+
+def fd_check_1d(s_factory, U0, tgt, n, K, dts, lam0, ndir: int = 32, eps: float = 1e-8):
+    """Directional derivatives of the 1D loss by central differences (dts
+    frozen) on `ndir` smooth random directions against the adjoint's."""
+    rng = np.random.default_rng(5)
+    x = (np.arange(n) + 0.5) / n
+    rel = []
+    for _ in range(ndir):
+        d = np.zeros_like(U0)
+        for k in range(3):
+            c = rng.standard_normal(4)
+            d[k, 2:-2] = sum(c[m] * np.sin(2 * np.pi * (m + 1) * x + c[(m + 1) % 4]) for m in range(4))
+        vals = []
+        for sgn in (1.0, -1.0):
+            s = s_factory()
+            s.freeze_dts(dts)
+            s.upload(U0 + sgn * eps * d)
+            s.step(K, 0.4)
+            r = s.download()[0, 2:-2] - tgt
+            vals.append(0.5 * float(np.sum(r * r)) / n)
+            s.close()
+        fd = (vals[0] - vals[1]) / (2 * eps)
+        ad = float(np.sum(lam0[:, 2:-2] * d[:, 2:-2]))
+        rel.append(abs(ad - fd) / max(abs(fd), 1e-300))
+    return {"directions": ndir, "eps": eps, "rel_err_median": float(np.median(rel)), "rel_err_max": float(np.max(rel))}
 
 
 def e2e_run(s, U, steps, cfl, st, cells, ws):

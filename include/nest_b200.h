@@ -276,6 +276,30 @@ nest_status nest_euler1d_run_noalloc(double* d_state, int n_interior, int n_halo
                                      int bc, double t_final, double cfl, int* steps_out, double* time_out,
                                      void* stream);
 
+/* ------------------------------------------------------------------------
+ * On-disk formats.
+ * nest's text snapshots, byte for byte the files its examples write for the
+ * same state and patch grid (replace write_output, examples/sod1d/sod1d.cpp:
+ * 50-91; write_output_2d and write_xslice, examples/sod2d/sod2d.cpp:58-152).
+ * U is a host array in the extended layout: 1D [3][n + 2 halo], 2D
+ * [4][nx + 4][ny + 4]; npatch / npx x npy is the patch grid that sets the
+ * order of the lines.  xslice = 1 writes the row j = ny / 2 sorted by x.
+ * ------------------------------------------------------------------------ */
+nest_status nest_write_dat_1d(const char* path, const double* U, int n, int halo, int npatch, double x_min,
+                              double x_max, double gamma, double time);
+nest_status nest_write_dat_2d(const char* path, const double* U, int nx, int ny, int npx, int npy, double x_min,
+                              double x_max, double y_min, double y_max, double gamma, double time, int xslice);
+/* The solver's current state and time (downloads; FP32 states are widened). */
+nest_status nest_solver_write_dat(nest_solver* s, const char* path, int npx, int npy, double x_min, double x_max,
+                                  double y_min, double y_max, int xslice);
+/* Restartable binary checkpoint (nest has none): state, time and step count,
+ * checksummed; loading into a solver of the same sizes, precision, boundary
+ * conditions, gamma and spacing continues the run bit for bit. */
+nest_status nest_solver_save(nest_solver* s, const char* path);
+nest_status nest_solver_load(nest_solver* s, const char* path);
+/* Set the solver clock (time, completed steps). */
+nest_status nest_solver_set_time(nest_solver* s, double time, int steps);
+
 #ifdef __cplusplus
 }
 #endif

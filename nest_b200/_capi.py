@@ -87,6 +87,12 @@ _SIGS = {
     "nest_solver_speed_slot": (_i, [_vp, C.POINTER(_vp)]),
     "nest_solver_stage_ptr": (_i, [_vp, C.POINTER(_vp)]),
     "nest_solver_stream": (_i, [_vp, C.POINTER(_vp)]),
+    "nest_solver_set_time": (_i, [_vp, _d, _i]),
+    "nest_write_dat_1d": (_i, [C.c_char_p, _vp, _i, _i, _i, _d, _d, _d, _d]),
+    "nest_write_dat_2d": (_i, [C.c_char_p, _vp, _i, _i, _i, _i, _d, _d, _d, _d, _d, _d, _i]),
+    "nest_solver_write_dat": (_i, [_vp, C.c_char_p, _i, _i, _d, _d, _d, _d, _i]),
+    "nest_solver_save": (_i, [_vp, C.c_char_p]),
+    "nest_solver_load": (_i, [_vp, C.c_char_p]),
     "nest_euler1d_run_noalloc": (_i, [_vp, _i, _i, _d, _d, _i, _d, _d, _ip, _dp, _vp]),
 }
 NOALLOC_MAX_CELLS = 65552

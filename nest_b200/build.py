@@ -36,6 +36,7 @@ UNITS = {
     "adjoint.cpp": ["-x", "cu"],
     "exchange.cu": [],
     "adjoint2d.cu": [],
+    "datio.cpp": ["-x", "cu", "-Xcompiler", "-ffp-contract=off"],
 }
 
 

@@ -450,13 +450,16 @@ nest_status nest_solver_time(nest_solver* s, double* time, int* steps) {
     return NEST_OK;
 }
 
-nest_status nest_solver_reset_time(nest_solver* s) {
+nest_status nest_solver_reset_time(nest_solver* s) { return nest_solver_set_time(s, 0.0, 0); }
+
+nest_status nest_solver_set_time(nest_solver* s, double time, int steps) {
     nest_status r = check(s);
     if (r != NEST_OK) return r;
+    if (!(time >= 0.0) || steps < 0) return fail(NEST_ERR_INVALID, "time and step count must be non-negative");
     CK(cudaStreamSynchronize(s->st));
     CK(cudaMemcpyAsync(s->host_ctrl, s->ctrl, sizeof(StepCtrl), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
-    for (int p = 0; p < 2; ++p) { s->host_ctrl->time[p] = 0.0; s->host_ctrl->step[p] = 0; }
+    for (int p = 0; p < 2; ++p) { s->host_ctrl->time[p] = time; s->host_ctrl->step[p] = steps; }
     CK(cudaMemcpyAsync(s->ctrl, s->host_ctrl, sizeof(StepCtrl), cudaMemcpyHostToDevice, s->st));
     CK(cudaStreamSynchronize(s->st));
     return NEST_OK;

@@ -2,6 +2,8 @@
 // Riemann solve and update in FP32; wave-speed maxima, totals, time and
 // positivity repair in FP64).  Compiled with FMA contraction and fast FP32
 // division / square root.
+#include <algorithm>
+
 #include "euler2d_kernels.cuh"
 #include "kernels.h"
 
@@ -17,7 +19,8 @@ __global__ void __launch_bounds__(256) k2d_prepare_f32(float* U, Geo2D g, StepCt
 }
 
 cudaError_t launch_2d_prepare_f32(float* U, const Geo2D& g, StepCtrl* ctrl, int p, cudaStream_t st) {
-    dim3 b(32, 8), gr((g.ny + 4 + 31) / 32, (g.nx + 4 + 7) / 8);
+    // rows folded per thread: about 16 (grid rows capped at 32 blocks)
+    dim3 b(32, 8), gr((g.ny + 4 + 31) / 32, std::min((g.nx + 4 + 7) / 8, 32));
     k2d_prepare_f32<<<gr, b, 0, st>>>(U, g, ctrl, p);
     return cudaGetLastError();
 }

@@ -308,8 +308,14 @@ __device__ __forceinline__ void x2_body(const StageArgs<float>& a, int strip, in
     }
 }
 
+#ifdef NEST_X2_MAXNREG
+#define NEST_X2_BOUNDS __maxnreg__(NEST_X2_MAXNREG)
+#else
+#define NEST_X2_BOUNDS __launch_bounds__(256)
+#endif
+
 template <int STAGE, bool REPAIR>
-__global__ void __launch_bounds__(256) k2d_f32x2(StageArgs<float> a) {
+__global__ void NEST_X2_BOUNDS k2d_f32x2(StageArgs<float> a) {
     x2_body<STAGE, REPAIR>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
 }
 

@@ -1,6 +1,8 @@
 // FP64 instantiation of the 2D stage kernels (the plain form).  Compiled with
 // -fmad=false and IEEE division / square root so that it reproduces the CPU
 // restatement of the scheme bit for bit.
+#include <algorithm>
+
 #include "euler2d_kernels.cuh"
 #include "kernels.h"
 
@@ -16,7 +18,8 @@ __global__ void __launch_bounds__(256) k2d_prepare_f64(double* U, Geo2D g, StepC
 }
 
 cudaError_t launch_2d_prepare_f64(double* U, const Geo2D& g, StepCtrl* ctrl, int p, cudaStream_t st) {
-    dim3 b(32, 8), gr((g.ny + 4 + 31) / 32, (g.nx + 4 + 7) / 8);
+    // rows folded per thread: about 16 (grid rows capped at 32 blocks)
+    dim3 b(32, 8), gr((g.ny + 4 + 31) / 32, std::min((g.nx + 4 + 7) / 8, 32));
     k2d_prepare_f64<<<gr, b, 0, st>>>(U, g, ctrl, p);
     return cudaGetLastError();
 }

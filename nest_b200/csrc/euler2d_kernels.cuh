@@ -415,15 +415,16 @@ struct BatchArgs {
 // into slot p.  Run once after an upload or an external state change.
 template <typename T>
 __device__ __forceinline__ void prepare2d_body(T* U, const Geo2D& g, StepCtrl* ctrl, int p) {
+    // Blocks of 32 x 8 threads: columns across a warp, rows strided by the grid's
+    // row extent, so each warp folds many cells before the block's one atomic pair.
     const T gamma = (T)g.gamma;
     const T gm1 = (T)(g.gamma - 1.0);
-    int j = blockIdx.x * blockDim.x + threadIdx.x;  // column in [-2, ny+2)
-    int i = blockIdx.y * blockDim.y + threadIdx.y;  // row in [-2, nx+2)
-    j -= 2; i -= 2;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x - 2;  // column in [-2, ny+2)
     double smx = 0.0, smy = 0.0;
-    bool in = (j >= -2 && j < g.ny + 2 && i >= -2 && i < g.nx + 2);
-    if ((i < 0 && g.xlo_ex) || (i >= g.nx && g.xhi_ex)) in = false;  // filled by the halo exchange
-    if (in) {
+    for (int i = blockIdx.y * blockDim.y + threadIdx.y - 2; i < g.nx + 2; i += gridDim.y * blockDim.y) {
+        bool in = (j >= -2 && j < g.ny + 2);
+        if ((i < 0 && g.xlo_ex) || (i >= g.nx && g.xhi_ex)) in = false;  // filled by the halo exchange
+        if (!in) continue;
         // source cell: wrap (periodic) or clamp (outflow) each axis
         int si = i, sj = j;
         if (i < 0 || i >= g.nx) si = (g.bcx == BC_PERIODIC) ? ((i + g.nx) % g.nx) : (i < 0 ? 0 : g.nx - 1);
@@ -434,14 +435,26 @@ __device__ __forceinline__ void prepare2d_body(T* U, const Geo2D& g, StepCtrl* c
             T sx, sy;
             long long o = g.at(i, j);
             cell_speeds<T>(U[o], U[g.vstride + o], U[2 * g.vstride + o], U[3 * g.vstride + o], gamma, gm1, sx, sy);
-            smx = sx; smy = sy;
+            smx = smax(smx, (double)sx);
+            smy = smax(smy, (double)sy);
         }
     }
     smx = warp_max(smx);
     smy = warp_max(smy);
-    if ((threadIdx.x & 31) == 0) {
-        atomic_max_speed(&ctrl->maxs[p][0], smx);
-        atomic_max_speed(&ctrl->maxs[p][1], smy);
+    __shared__ double red[2][32];
+    const int w = (threadIdx.y * blockDim.x + threadIdx.x) >> 5, nw = (blockDim.x * blockDim.y) >> 5;
+    if ((threadIdx.x & 31) == 0) { red[0][w] = smx; red[1][w] = smy; }
+    __syncthreads();
+    if (w == 0) {
+        const int l = threadIdx.x & 31;
+        smx = l < nw ? red[0][l] : 0.0;
+        smy = l < nw ? red[1][l] : 0.0;
+        smx = warp_max(smx);
+        smy = warp_max(smy);
+        if (l == 0) {
+            atomic_max_speed(&ctrl->maxs[p][0], smx);
+            atomic_max_speed(&ctrl->maxs[p][1], smy);
+        }
     }
 }
 

@@ -219,3 +219,23 @@ class Solver:
         p = C.c_void_p()
         check(lib.nest_solver_stream(self._h, C.byref(p)), "nest_solver_stream")
         return p.value or 0
+
+    # -- on-disk formats ------------------------------------------------------
+    def write_dat(self, path, npx: int = 1, npy: int = 1, x_min: float = 0.0, x_max: float = 1.0,
+                  y_min: float = 0.0, y_max: float = 1.0, xslice: bool = False):
+        """nest's text snapshot of the current state and time (patch grid npx x npy)."""
+        import os
+        check(lib.nest_solver_write_dat(self._h, os.fsencode(path), npx, npy, x_min, x_max, y_min, y_max,
+                                        int(xslice)), "nest_solver_write_dat")
+
+    def save(self, path):
+        """Restartable checkpoint: state, time and step count."""
+        import os
+        check(lib.nest_solver_save(self._h, os.fsencode(path)), "nest_solver_save")
+
+    def load(self, path):
+        import os
+        check(lib.nest_solver_load(self._h, os.fsencode(path)), "nest_solver_load")
+
+    def set_time(self, time: float, steps: int = 0):
+        check(lib.nest_solver_set_time(self._h, time, steps), "nest_solver_set_time")

@@ -202,11 +202,35 @@ class Reference:
             "ref_sod1d_main": (i, []),
             "ref_sod2d_main": (i, []),
             "ref_run_cpu_sod": (None, [i, d, d, _dp]),
+            "ref_write_sod1d": (None, [_dp, i, i, i, d, d, d, d, i]),
+            "ref_write_sod2d": (None, [_dp, i, i, i, i, d, d, d, d, d, d, i]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
+
+    def write_sod1d(self, directory, U, n, halo, npatch, x_min, x_max, gamma, time, step):
+        """nest's write_output on state U; returns the path of the file it wrote."""
+        U = np.ascontiguousarray(U, np.float64)
+        cwd = os.getcwd()
+        os.chdir(directory)
+        try:
+            self.L.ref_write_sod1d(_ptr(U), n, halo, npatch, x_min, x_max, gamma, time, step)
+        finally:
+            os.chdir(cwd)
+        return Path(directory) / f"sod_{step:04d}.dat"
+
+    def write_sod2d(self, directory, U, nx, ny, npx, npy, x_min, x_max, y_min, y_max, gamma, time, step):
+        """nest's write_output_2d and write_xslice; returns both paths."""
+        U = np.ascontiguousarray(U, np.float64)
+        cwd = os.getcwd()
+        os.chdir(directory)
+        try:
+            self.L.ref_write_sod2d(_ptr(U), nx, ny, npx, npy, x_min, x_max, y_min, y_max, gamma, time, step)
+        finally:
+            os.chdir(cwd)
+        return Path(directory) / f"sod2d_{step:04d}.dat", Path(directory) / f"sod2d_xslice_{step:04d}.dat"
 
     def hlle_flux(self, gamma, WL, WR):
         F = np.zeros(3)
