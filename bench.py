@@ -208,6 +208,11 @@ def alg_bytes_per_cell(form: str):
     return {"stage1": 8 * s, "stage2": 12 * s, "per_cell_update": 10 * s}
 
 
+def kernel_name(form: str, stage: str) -> str:
+    """Name of the stage kernel the bench's form launches (no repair flag)."""
+    return ("k2d_f32x2_" if form == "f32" else "k2d_f64_") + stage[-1]
+
+
 def traffic_from_profiles(form: str, n: int):
     f = ROOT / "profiles" / "traffic.json"
     if not f.exists():
@@ -339,7 +344,7 @@ def run_ours(args, ws, rank, local):
                 "tiling": {"rows_per_tile": r["tiling"][0], "warps_per_block": r["tiling"][1]},
                 "kernel_ms": {"stage1": m1, "stage2": m2},
                 "hbm_gbs_step": value / ws * ab["per_cell_update"] / 1e9,
-                "roofline": {"bound": "hbm", "kernel": f"k2d_{form}<{dom[-1]}>", "achieved": achieved, "peak": hbm,
+                "roofline": {"bound": "hbm", "kernel": kernel_name(form, dom), "achieved": achieved, "peak": hbm,
                              "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
                              "alg_bytes_per_launch": ab[dom] * cl, "traffic": (tr or {}).get(dom)},
                 "window": r["window"],
@@ -390,7 +395,7 @@ def run_ours(args, ws, rank, local):
             "sim_time": tsim, "steps": nst, "tiling": {"rows_per_tile": tiling[0], "warps_per_block": tiling[1]},
             "kernel_ms": {"stage1": m1, "stage2": m2},
             "hbm_gbs_step": value / ws * ab["per_cell_update"] / 1e9,
-            "roofline": {"bound": "hbm", "kernel": f"k2d_{form}<{dom[-1]}>", "achieved": achieved, "peak": hbm,
+            "roofline": {"bound": "hbm", "kernel": kernel_name(form, dom), "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": ab[dom] * cells,
                          "traffic": (tr or {}).get(dom)},

@@ -51,8 +51,12 @@ enum {
     NEST_FLAG_REPAIR = 2,       /* FP32 form: FP64 positivity repair near vacuum */
     NEST_FLAG_NO_RESIDENT = 4,  /* 1D: never use the single-CTA resident solver */
     NEST_FLAG_FP32_SCALAR = 8,  /* FP32 form: one column per lane instead of packed FP32x2 pairs */
-    NEST_FLAG_SPLIT_COMPAT = 16 /* 2D FP64: nest's own dimensionally split forward-Euler sweeps
+    NEST_FLAG_SPLIT_COMPAT = 16, /* 2D FP64: nest's own dimensionally split forward-Euler sweeps
                                    (examples/sod2d/euler2d.hpp:67-271) instead of unsplit RK2 */
+    NEST_FLAG_LIMITER_MC = 32,   /* slope limiter: monotonized central (mc_limiter, euler1d.hpp:117-125) */
+    NEST_FLAG_LIMITER_NONE = 64  /* slope limiter: none, 0.5 (left + right) (apply_limiter, euler1d.hpp:127-137);
+                                    default minmod.  The packed FP32 kernel is minmod-only: FP32 solvers
+                                    with another limiter run the one-column-per-lane kernel. */
 };
 
 /* ------------------------------------------------------------------------ */

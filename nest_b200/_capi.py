@@ -22,6 +22,7 @@ BC_PERIODIC, BC_OUTFLOW = 0, 1
 F64, F32 = 0, 1
 LAYOUT_EXTENDED, LAYOUT_INTERIOR = 0, 1
 FLAG_TOTALS, FLAG_REPAIR, FLAG_NO_RESIDENT, FLAG_FP32_SCALAR, FLAG_SPLIT_COMPAT = 1, 2, 4, 8, 16
+FLAG_LIMITER_MC, FLAG_LIMITER_NONE = 32, 64
 
 
 class NestError(RuntimeError):

@@ -272,6 +272,8 @@ nest_status nest_adjoint_create(nest_solver* s, int nsteps, int policy, int para
         return fail(NEST_ERR_UNSUPPORTED, "adjoint: periodic boundaries");
     if (s->d.flags & (NEST_FLAG_SPLIT_COMPAT | NEST_FLAG_FP32_SCALAR))
         return fail(NEST_ERR_UNSUPPORTED, "adjoint: unsplit RK2 scheme only");
+    if (s->d.flags & (NEST_FLAG_LIMITER_MC | NEST_FLAG_LIMITER_NONE))
+        return fail(NEST_ERR_UNSUPPORTED, "adjoint: minmod limiter only");
     auto* a = new (std::nothrow) nest_adjoint;
     if (!a) return fail(NEST_ERR_OOM, "host allocation failed");
     a->s = s;

@@ -57,6 +57,7 @@ nest_status drop_graphs(nest_solver* s) {
 
 LoopParams base_params(const nest_solver* s) {
     LoopParams lp{};
+    lp.lim = (s->d.flags & NEST_FLAG_LIMITER_MC) ? LIM_MC : (s->d.flags & NEST_FLAG_LIMITER_NONE) ? LIM_NONE : LIM_MINMOD;
     lp.dts_in = (s->dts_mode == 0) ? s->dts_in : nullptr;
     lp.dts_out = (s->dts_mode == 1) ? s->dts_out : nullptr;
     lp.dts_cap = s->dts_cap;
@@ -91,7 +92,7 @@ cudaError_t nestb::rt::enqueue_step(nest_solver* s, const LoopParams& lp, int p,
     if (s->d.precision == NEST_F64)
         return launch_2d_step_f64((double*)s->U, (double*)s->U1, s->geo(), lp, s->ctrl, s->partials, p, s->tx,
                                   s->warps, which, s->st);
-    if (s->d.flags & NEST_FLAG_FP32_SCALAR)
+    if (s->d.flags & (NEST_FLAG_FP32_SCALAR | NEST_FLAG_LIMITER_MC | NEST_FLAG_LIMITER_NONE))
         return launch_2d_step_f32((float*)s->U, (float*)s->U1, s->geo(), lp, s->ctrl, s->partials, p, s->tx,
                                   s->warps, (s->d.flags & NEST_FLAG_REPAIR) != 0, which, s->st);
     return launch_2d_step_f32x2((float*)s->U, (float*)s->U1, s->geo(), lp, s->ctrl, s->partials, p, s->tx,
@@ -232,6 +233,8 @@ nest_status nest_solver_create(const nest_solver_desc* d, nest_solver** out) {
         return fail(NEST_ERR_UNSUPPORTED, "nest's split scheme runs in 2D FP64");
     if ((d->flags & NEST_FLAG_SPLIT_COMPAT) && (d->flags & NEST_FLAG_TOTALS))
         return fail(NEST_ERR_UNSUPPORTED, "totals are kept by the RK2 scheme only");
+    if ((d->flags & NEST_FLAG_LIMITER_MC) && (d->flags & NEST_FLAG_LIMITER_NONE))
+        return fail(NEST_ERR_INVALID, "choose one slope limiter");
 
     nest_solver* s = new (std::nothrow) nest_solver;
     if (!s) return fail(NEST_ERR_OOM, "host allocation failed");
@@ -798,6 +801,8 @@ nest_status nest_batch_create(const nest_batch_desc* d, nest_batch** out) {
     if (!(d->gamma > 1.0)) return fail(NEST_ERR_INVALID, "gamma must exceed 1");
     if (d->bc_x != NEST_BC_PERIODIC && d->bc_x != NEST_BC_OUTFLOW) return fail(NEST_ERR_INVALID, "bad bc_x");
     if (d->bc_y != NEST_BC_PERIODIC && d->bc_y != NEST_BC_OUTFLOW) return fail(NEST_ERR_INVALID, "bad bc_y");
+    if (d->flags & (NEST_FLAG_LIMITER_MC | NEST_FLAG_LIMITER_NONE))
+        return fail(NEST_ERR_UNSUPPORTED, "batched problems use the minmod limiter");
     for (int p = 0; p < d->count; ++p)
         if (d->nx[p] < 4 || d->ny[p] < 4) return fail(NEST_ERR_INVALID, "every problem needs >= 4 cells per axis");
     nest_batch* b = new (std::nothrow) nest_batch;

@@ -51,7 +51,10 @@ struct LoopParams {
     int dts_cap;           // capacity of dts_in / dts_out
     double fixed_dt;       // > 0: every step uses this dt (nest's rk2_step(dt))
     int step_budget;       // resident 1D kernel: > 0 = at most this many steps per launch
+    int lim;               // slope limiter: LIM_MINMOD, LIM_MC or LIM_NONE
 };
+
+enum { LIM_MINMOD = 0, LIM_MC = 1, LIM_NONE = 2 };
 
 // std::min / std::max semantics (first argument wins ties).
 template <typename T> __device__ __forceinline__ T smin(T a, T b) { return (b < a) ? b : a; }
@@ -142,6 +145,18 @@ template <typename T>
 __device__ __forceinline__ T minmod(T a, T b) {
     if (a * b <= T(0)) return T(0);
     return (fabs(a) < fabs(b)) ? a : b;
+}
+
+// apply_limiter, euler1d.hpp:127-137 (mc_limiter = minmod3(2a, (a+b)/2, 2b),
+// euler1d.hpp:117-125).  `lim` is uniform across a launch.
+template <typename T>
+__device__ __forceinline__ T limit(T a, T b, int lim) {
+    if (lim == LIM_MINMOD) return minmod(a, b);
+    if (lim == LIM_MC) {
+        T c = T(0.5) * (a + b);
+        return minmod(T(2) * a, minmod(c, T(2) * b));
+    }
+    return T(0.5) * (a + b);
 }
 
 // hlle_flux, euler1d.hpp:178-242 (Davis speeds, three branches).

@@ -51,7 +51,7 @@ __device__ double block_max_1d(double v, double* red) {
 // arrays of 3*nt; W scratch 3*nt; F scratch 3*(n+1).  If avg != nullptr the
 // result is 0.5*(avg + stage) (second Heun stage, written into avg).
 __device__ void resident_stage(const double* Uin, double* Uout, double* avg, double* W, double* F,
-                               int n, int h, double dtdx, double gamma, double gm1) {
+                               int n, int h, double dtdx, double gamma, double gm1, int lim) {
     int nt = n + 2 * h;
     for (int f = threadIdx.x; f <= n; f += blockDim.x) {
         // face between extended cells a = h+f-1 and b = h+f
@@ -60,8 +60,8 @@ __device__ void resident_stage(const double* Uin, double* Uout, double* avg, dou
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const double* w = W + k * nt;
-            sa[k] = minmod(w[a] - w[a - 1], w[b] - w[a]);
-            sb[k] = minmod(w[b] - w[a], w[b + 1] - w[b]);
+            sa[k] = limit(w[a] - w[a - 1], w[b] - w[a], lim);
+            sb[k] = limit(w[b] - w[a], w[b + 1] - w[b], lim);
         }
         double rL = W[a] + 0.5 * sa[0], uL = W[nt + a] + 0.5 * sa[1], pL = W[2 * nt + a] + 0.5 * sa[2];
         double rR = W[b] - 0.5 * sb[0], uR = W[nt + b] - 0.5 * sb[1], pR = W[2 * nt + b] - 0.5 * sb[2];
@@ -145,12 +145,12 @@ k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int
         if (!(ms == ms) || ms > 1.79e308) { if (threadIdx.x == 0) atomicOr(&ctrl->err, ERRW_NONFINITE); break; }
         if (threadIdx.x == 0 && lp.dts_out && step < lp.dts_cap) lp.dts_out[step] = dt;
         double dtdx = dt / dx;
-        resident_stage(U, U1, nullptr, W, F, n, h, dtdx, gamma, gm1);
+        resident_stage(U, U1, nullptr, W, F, n, h, dtdx, gamma, gm1, lp.lim);
         // Stage 2 on U1, averaged into U.
         resident_ghosts(U1, n, h, bc);
         resident_prims(U1, W, n, h, gamma, gm1);
         __syncthreads();
-        resident_stage(U1, nullptr, U, W, F, n, h, dtdx, gamma, gm1);
+        resident_stage(U1, nullptr, U, W, F, n, h, dtdx, gamma, gm1, lp.lim);
         time += dt;
         ++step;
     }
@@ -245,8 +245,8 @@ k1d_stage(const double* __restrict__ Uin, const double* Un, double* Uout,
         double sa[3], sb[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            sa[k] = minmod(W[k][a] - W[k][a - 1], W[k][b] - W[k][a]);
-            sb[k] = minmod(W[k][b] - W[k][a], W[k][b + 1] - W[k][b]);
+            sa[k] = limit(W[k][a] - W[k][a - 1], W[k][b] - W[k][a], lp.lim);
+            sb[k] = limit(W[k][b] - W[k][a], W[k][b + 1] - W[k][b], lp.lim);
         }
         double f0, f1, f2;
         hlle1d(gamma, gm1, W[0][a] + 0.5 * sa[0], W[1][a] + 0.5 * sa[1], W[2][a] + 0.5 * sa[2],

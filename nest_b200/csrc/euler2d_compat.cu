@@ -50,22 +50,23 @@ __device__ __forceinline__ double iface_velocity(double uL, double uR, double cL
 // passive_flux, euler2d.hpp:31-33.
 __device__ __forceinline__ double passive(double qL, double qR, double u) { return (u >= 0.0) ? u * qL : u * qR; }
 
-// Flux of one face from the four cells m2, m1 | p0, p1 (plm_reconstruct,
+// Flux of one face from the four cells m2, m1 | p0, p1 (plm_reconstruct with
+// nest's limiter choice,
 // euler1d.hpp:149-171, then hlle_flux, euler1d.hpp:178-242, and the passive
 // transverse flux).  f[0..2]: (rho, normal momentum, E); f[3]: transverse.
 __device__ __forceinline__ void compat_face(const P3& m2, const P3& m1, const P3& p0, const P3& p1, double gamma,
-                                            double gm1, double f[4]) {
-    double sa0 = minmod(m1.r - m2.r, p0.r - m1.r), sa1 = minmod(m1.u - m2.u, p0.u - m1.u),
-           sa2 = minmod(m1.p - m2.p, p0.p - m1.p);
-    double sb0 = minmod(p0.r - m1.r, p1.r - p0.r), sb1 = minmod(p0.u - m1.u, p1.u - p0.u),
-           sb2 = minmod(p0.p - m1.p, p1.p - p0.p);
+                                            double gm1, int lim, double f[4]) {
+    double sa0 = limit(m1.r - m2.r, p0.r - m1.r, lim), sa1 = limit(m1.u - m2.u, p0.u - m1.u, lim),
+           sa2 = limit(m1.p - m2.p, p0.p - m1.p, lim);
+    double sb0 = limit(p0.r - m1.r, p1.r - p0.r, lim), sb1 = limit(p0.u - m1.u, p1.u - p0.u, lim),
+           sb2 = limit(p0.p - m1.p, p1.p - p0.p, lim);
     double rL = m1.r + 0.5 * sa0, uL = m1.u + 0.5 * sa1, pL = m1.p + 0.5 * sa2;
     double rR = p0.r - 0.5 * sb0, uR = p0.u - 0.5 * sb1, pR = p0.p - 0.5 * sb2;
     hlle1d(gamma, gm1, rL, uL, pL, rR, uR, pR, f[0], f[1], f[2]);
     double cL = sqrt(gamma * pL / rL), cR = sqrt(gamma * pR / rR);
     double ui = iface_velocity(uL, uR, cL, cR);
-    double qL = m1.q + 0.5 * minmod(m1.q - m2.q, p0.q - m1.q);
-    double qR = p0.q - 0.5 * minmod(p0.q - m1.q, p1.q - p0.q);
+    double qL = m1.q + 0.5 * limit(m1.q - m2.q, p0.q - m1.q, lim);
+    double qR = p0.q - 0.5 * limit(p0.q - m1.q, p1.q - p0.q, lim);
     f[3] = passive(qL, qR, ui);
 }
 
@@ -101,8 +102,8 @@ __global__ void __launch_bounds__(256) k2d_compat_sweep(const double* __restrict
         P3 w[5];
         for (int k = 0; k < 5; ++k) w[k] = prim_compat(Uin, vs, o + (k - 2) * st, XDIR, gm1);
         double fL[4], fR[4];
-        compat_face(w[0], w[1], w[2], w[3], gamma, gm1, fL);
-        compat_face(w[1], w[2], w[3], w[4], gamma, gm1, fR);
+        compat_face(w[0], w[1], w[2], w[3], gamma, gm1, lp.lim, fL);
+        compat_face(w[1], w[2], w[3], w[4], gamma, gm1, lp.lim, fR);
         double dtd = dt / (XDIR ? g.dx : g.dy);
         double v0 = Uin[o] - dtd * (fR[0] - fL[0]);
         double vn = Uin[(XDIR ? 1 : 2) * vs + o] - dtd * (fR[1] - fL[1]);

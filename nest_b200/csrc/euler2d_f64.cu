@@ -8,9 +8,29 @@
 
 namespace nestb {
 
-template <int STAGE>
-__global__ void __launch_bounds__(256) k2d_f64(StageArgs<double> a) {
-    stage2d_body<double, STAGE, false>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+// Register budgets of the two stage kernels (0: ptxas's choice).
+#ifndef NEST_F64_REGS1
+#define NEST_F64_REGS1 0
+#endif
+#ifndef NEST_F64_REGS2
+#define NEST_F64_REGS2 0
+#endif
+#if NEST_F64_REGS1 > 0
+#define NEST_F64_ATTR1 __maxnreg__(NEST_F64_REGS1)
+#else
+#define NEST_F64_ATTR1 __launch_bounds__(256)
+#endif
+#if NEST_F64_REGS2 > 0
+#define NEST_F64_ATTR2 __maxnreg__(NEST_F64_REGS2)
+#else
+#define NEST_F64_ATTR2 __launch_bounds__(256)
+#endif
+
+__global__ void NEST_F64_ATTR1 k2d_f64_1(StageArgs<double> a) {
+    stage2d_body<double, 1, false>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+}
+__global__ void NEST_F64_ATTR2 k2d_f64_2(StageArgs<double> a) {
+    stage2d_body<double, 2, false>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
 }
 
 __global__ void __launch_bounds__(256) k2d_prepare_f64(double* U, Geo2D g, StepCtrl* ctrl, int p) {
@@ -30,9 +50,9 @@ cudaError_t launch_2d_step_f64(double* U, double* U1, const Geo2D& g, const Loop
     int nstrips = (g.ny + STRIP - 1) / STRIP;
     dim3 b(32, warps), gr((nstrips + warps - 1) / warps, (g.nx + tx - 1) / tx);
     StageArgs<double> a1{U, nullptr, U1, g, lp, ctrl, nullptr, p, tx};
-    if (which & 1) k2d_f64<1><<<gr, b, 0, st>>>(a1);
+    if (which & 1) k2d_f64_1<<<gr, b, 0, st>>>(a1);
     StageArgs<double> a2{U1, U, Uout ? Uout : U, g, lp, ctrl, partials, p, tx};
-    if (which & 2) k2d_f64<2><<<gr, b, 0, st>>>(a2);
+    if (which & 2) k2d_f64_2<<<gr, b, 0, st>>>(a2);
     return cudaGetLastError();
 }
 

@@ -208,9 +208,9 @@ template <typename T>
 __device__ __forceinline__ Win4<T> prim_win(const Prim4<T>& w) { return { w.r, w.u, w.v, w.p }; }
 
 template <typename T>
-__device__ __forceinline__ Win4<T> minmod4(const Win4<T>& m, const Win4<T>& o, const Win4<T>& p) {
-    return { minmod(o.a - m.a, p.a - o.a), minmod(o.b - m.b, p.b - o.b),
-             minmod(o.c - m.c, p.c - o.c), minmod(o.d - m.d, p.d - o.d) };
+__device__ __forceinline__ Win4<T> limit4(const Win4<T>& m, const Win4<T>& o, const Win4<T>& p, int lim) {
+    return { limit(o.a - m.a, p.a - o.a, lim), limit(o.b - m.b, p.b - o.b, lim),
+             limit(o.c - m.c, p.c - o.c, lim), limit(o.d - m.d, p.d - o.d, lim) };
 }
 
 // Per-launch arguments of a stage kernel.
@@ -298,7 +298,7 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
         W0 = W1; W1 = W2; W2 = prim_win(w);
         if (r >= 0) {
             S0 = S1;
-            S1 = minmod4(W0, W1, W2);  // slope of row r-1
+            S1 = limit4(W0, W1, W2, a.lp.lim);  // slope of row r-1
         }
         if (r >= 1) {
             // x-face between rows r-2 and r-1 (normal u, transverse v)
@@ -312,7 +312,7 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
                 const int i = i0 + r - 2;
                 // y-direction on row q (window W0): slopes, faces, neighbours
                 Win4<T> Wl = shfl_up4(W0), Wr = shfl_dn4(W0);
-                Win4<T> sy = minmod4(Wl, W0, Wr);
+                Win4<T> sy = limit4(Wl, W0, Wr, a.lp.lim);
                 Win4<T> Mq = { W0.a - T(0.5) * sy.a, W0.b - T(0.5) * sy.b, W0.c - T(0.5) * sy.c, W0.d - T(0.5) * sy.d };
                 Win4<T> Rq = shfl_dn4(Mq);
                 Win4<T> Gy;  // face j+1/2: normal v, transverse u

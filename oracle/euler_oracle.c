@@ -185,6 +185,13 @@ void orc1d_fill_ghosts(double* U, int n, int h, int bc) {
     }
 }
 
+/* Slope limiter of the stage functions below (minmod unless set; the
+ * OpenMP path of benchmark_euler1d.cpp:145-154 is minmod, nest's sweeps and
+ * plm_reconstruct take any limiter_t).  Process-wide: not for concurrent use
+ * with different limiters. */
+static int g_lim = ORC_LIM_MINMOD;
+void orc_set_limiter(int lim) { g_lim = lim; }
+
 /* One forward-Euler stage U_out = U_in - dt/dx (F_{i+1/2} - F_{i-1/2}) on
  * the interior: the compute_rhs lambda, benchmark_euler1d.cpp:113-165
  * (cons->prim over n_total 116-125, PLM 145-154, two HLLE 156-158,
@@ -207,9 +214,9 @@ void orc1d_stage(const double* Uin, double* Uout, double* W, int n, int h,
         }
         double WLm[3], WRm[3], WLp[3], WRp[3];
         for (int k = 0; k < 3; ++k) {
-            double s_im1 = orc_minmod(Wm1[k] - Wm2[k], W0[k] - Wm1[k]);
-            double s_i = orc_minmod(W0[k] - Wm1[k], Wp1[k] - W0[k]);
-            double s_ip1 = orc_minmod(Wp1[k] - W0[k], Wp2[k] - Wp1[k]);
+            double s_im1 = orc_limit(Wm1[k] - Wm2[k], W0[k] - Wm1[k], g_lim);
+            double s_i = orc_limit(W0[k] - Wm1[k], Wp1[k] - W0[k], g_lim);
+            double s_ip1 = orc_limit(Wp1[k] - W0[k], Wp2[k] - Wp1[k], g_lim);
             WLm[k] = Wm1[k] + 0.5 * s_im1;
             WRm[k] = W0[k] - 0.5 * s_i;
             WLp[k] = W0[k] + 0.5 * s_i;
@@ -429,8 +436,8 @@ static void face_flux(const double* W, size_t plane, size_t a2, size_t a, size_t
     w_at(W, plane, a2, xdir, Wa2); w_at(W, plane, a, xdir, Wa);
     w_at(W, plane, b, xdir, Wb);   w_at(W, plane, b2, xdir, Wb2);
     for (int k = 0; k < 4; ++k) {
-        double sa = orc_minmod(Wa[k] - Wa2[k], Wb[k] - Wa[k]);
-        double sb = orc_minmod(Wb[k] - Wa[k], Wb2[k] - Wb[k]);
+        double sa = orc_limit(Wa[k] - Wa2[k], Wb[k] - Wa[k], g_lim);
+        double sb = orc_limit(Wb[k] - Wa[k], Wb2[k] - Wb[k], g_lim);
         WLf[k] = Wa[k] + 0.5 * sa;
         WRf[k] = Wb[k] - 0.5 * sb;
     }

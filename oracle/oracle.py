@@ -51,6 +51,7 @@ class Oracle:
         d, i = C.c_double, C.c_int
         sig = {
             "orc_set_threads": (None, [i]),
+            "orc_set_limiter": (None, [i]),
             "orc_max_threads": (i, []),
             "orc_pressure": (d, [d, d, d, d]),
             "orc_total_energy": (d, [d, d, d, d]),
@@ -83,6 +84,10 @@ class Oracle:
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
+
+    def set_limiter(self, lim: int) -> None:
+        """Limiter of the stage functions: 0 minmod (default), 1 MC, 2 none."""
+        self.L.orc_set_limiter(int(lim))
 
     def set_threads(self, n: int) -> None:
         self.L.orc_set_threads(int(n))
@@ -195,8 +200,8 @@ class Reference:
             "ref_exchange_1d": (i, [_dp, i, i, i, i]),
             "ref_exchange_2d": (i, [_dp, i, i, i, i, i, i]),
             "ref_patch_boxes_2d": (i, [i, i, i, i, _ip]),
-            "ref_x_sweep": (None, [_dp, _dp, i, i, i, d, d, d]),
-            "ref_y_sweep": (None, [_dp, _dp, i, i, i, d, d, d]),
+            "ref_x_sweep": (None, [_dp, _dp, i, i, i, d, d, d, i]),
+            "ref_y_sweep": (None, [_dp, _dp, i, i, i, d, d, d, i]),
             "ref_compute_dt_2d": (d, [_dp, i, i, i, d, d, d, d]),
             "ref_benchmark_cpu": (d, [i, d, _ip, _dp]),
             "ref_sod1d_main": (i, []),

@@ -118,31 +118,36 @@ int ref_patch_boxes_2d(int nx, int ny, int npx, int npy, int* boxes) {
     return k;
 }
 
+// limiter_t from an integer: 0 minmod, 1 MC, 2 none (euler1d.hpp:106-110).
+static limiter_t ref_limiter(int lim) {
+    return lim == 1 ? limiter_t::mc : (lim == 2 ? limiter_t::none : limiter_t::minmod);
+}
+
 // The reference's dimensionally split 2D sweeps (euler2d.hpp:67-239) and
 // CFL (euler2d.hpp:242-271) on a single patch whose ghost ring is already
 // filled.  Layout: SoA over the extended space, y fastest.
 void ref_x_sweep(const double* Uin, double* Uout, int nx, int ny, int h, double dx,
-                 double dt, double gamma) {
+                 double dt, double gamma, int lim) {
     auto interior = index_space(ivec(0, 0), uvec(static_cast<unsigned>(nx), static_cast<unsigned>(ny)));
     auto extended = expand(interior, h);
     std::size_t nt = size(extended);
     std::vector<double> in(Uin, Uin + 4 * nt), out(Uin, Uin + 4 * nt);
     field_t<double, 2> fin(in.data(), 4, extended), fout(out.data(), 4, extended);
     eos_t eos{gamma};
-    euler2d::x_sweep_t sweep(eos, dx, limiter_t::minmod);
+    euler2d::x_sweep_t sweep(eos, dx, ref_limiter(lim));
     sweep(fin, fout, interior, dt);
     for (std::size_t i = 0; i < 4 * nt; ++i) Uout[i] = out[i];
 }
 
 void ref_y_sweep(const double* Uin, double* Uout, int nx, int ny, int h, double dy,
-                 double dt, double gamma) {
+                 double dt, double gamma, int lim) {
     auto interior = index_space(ivec(0, 0), uvec(static_cast<unsigned>(nx), static_cast<unsigned>(ny)));
     auto extended = expand(interior, h);
     std::size_t nt = size(extended);
     std::vector<double> in(Uin, Uin + 4 * nt), out(Uin, Uin + 4 * nt);
     field_t<double, 2> fin(in.data(), 4, extended), fout(out.data(), 4, extended);
     eos_t eos{gamma};
-    euler2d::y_sweep_t sweep(eos, dy, limiter_t::minmod);
+    euler2d::y_sweep_t sweep(eos, dy, ref_limiter(lim));
     sweep(fin, fout, interior, dt);
     for (std::size_t i = 0; i < 4 * nt; ++i) Uout[i] = out[i];
 }

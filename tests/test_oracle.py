@@ -183,9 +183,10 @@ def test_2d_periodic_conserves_mass(oracle):
     assert abs(m1[3] - m0[3]) < 1e-13 * abs(m0[3])
 
 
-def sod2d_reference_run(ref, oracle):
+def sod2d_reference_run(ref, oracle, lim=0):
     """nest's sod2d (examples/sod2d/sod2d.cpp:239-366) on one periodic domain
-    with nest's own x_sweep_t / y_sweep_t / compute_dt_2d from oracle/_ref."""
+    with nest's own x_sweep_t / y_sweep_t / compute_dt_2d from oracle/_ref
+    (lim: 0 minmod as in sod2d, 1 MC, 2 none)."""
     import ctypes as C
     nx, ny, tf, cfl = 200, 20, 0.2, 0.3
     dx, dy = 1.0 / nx, 0.1 / ny
@@ -203,7 +204,7 @@ def sod2d_reference_run(ref, oracle):
         for sweep, d in ((ref.L.ref_x_sweep, dx), (ref.L.ref_y_sweep, dy)):
             oracle.fill_ghosts2d(U, nx, ny, 2, BC_PERIODIC)
             out = np.empty_like(U)
-            sweep(U.ctypes.data_as(dp), out.ctypes.data_as(dp), nx, ny, 2, d, dt, G)
+            sweep(U.ctypes.data_as(dp), out.ctypes.data_as(dp), nx, ny, 2, d, dt, G, lim)
             U = out
         t += dt
         steps += 1
