@@ -30,8 +30,9 @@ struct St3 { double r, u, p; };
 // Reverse of hlle1d (common.cuh) for one face: accumulates Wbar of the left
 // and right face states for the flux adjoint fb.
 __device__ void hlle1d_adj(double gamma, double gm1, St3 L, St3 R, const double fb[3], double wl[3], double wr[3]) {
+    const double igm1 = 1.0 / gm1;
     double cL = sqrt(gamma * L.p / L.r), cR = sqrt(gamma * R.p / R.r);
-    double EL = L.p / gm1 + 0.5 * L.r * L.u * L.u, ER = R.p / gm1 + 0.5 * R.r * R.u * R.u;
+    double EL = L.p * igm1 + 0.5 * L.r * L.u * L.u, ER = R.p * igm1 + 0.5 * R.r * R.u * R.u;
     double aL = L.u - cL, aR = R.u - cR;
     double bL = L.u + cL, bR = R.u + cR;
     double SL = smin(aL, aR), SR = smax(bL, bR);
@@ -47,16 +48,19 @@ __device__ void hlle1d_adj(double gamma, double gm1, St3 L, St3 R, const double 
     } else if (SR <= 0.0) {
         for (int k = 0; k < 3; ++k) fRb[k] = fb[k];
     } else {
-        double D = SR - SL;
+        // one reciprocal per face: the adjoint needs the derivative, not the
+        // forward's rounding
+        const double iD = 1.0 / (SR - SL);
         for (int k = 0; k < 3; ++k) {
             double dU = UR[k] - UL[k];
-            double F = (SR * FL[k] - SL * FR[k] + SL * SR * dU) / D;
-            fLb[k] = fb[k] * SR / D;
-            fRb[k] = -fb[k] * SL / D;
-            uRb[k] = fb[k] * SL * SR / D;
+            double F = (SR * FL[k] - SL * FR[k] + SL * SR * dU) * iD;
+            double g = fb[k] * iD;
+            fLb[k] = g * SR;
+            fRb[k] = -g * SL;
+            uRb[k] = g * SL * SR;
             uLb[k] = -uRb[k];
-            SLb += fb[k] * (-FR[k] + SR * dU + F) / D;
-            SRb += fb[k] * (FL[k] + SL * dU - F) / D;
+            SLb += g * (-FR[k] + SR * dU + F);
+            SRb += g * (FL[k] + SL * dU - F);
         }
     }
     // Davis speeds -> u and c of the active side
@@ -76,9 +80,13 @@ __device__ void hlle1d_adj(double gamma, double gm1, St3 L, St3 R, const double 
         // U = (r, r u, E)
         rb += ub_[0]; rb += ub_[1] * S.u; ub += ub_[1] * S.r; Eb += ub_[2];
         // E = p / (g-1) + 0.5 r u^2
-        pb += Eb / gm1; rb += Eb * 0.5 * S.u * S.u; ub += Eb * S.r * S.u;
-        // c = sqrt(g p / r)
-        if (c > 0.0) { pb += cbar * gamma / (2.0 * S.r * c); rb -= cbar * c / (2.0 * S.r); }
+        pb += Eb * igm1; rb += Eb * 0.5 * S.u * S.u; ub += Eb * S.r * S.u;
+        // c = sqrt(g p / r): dc/dp = g / (2 r c), dc/dr = -c / (2 r)
+        if (c > 0.0) {
+            const double i2r = 0.5 / S.r;
+            pb += cbar * gamma * i2r / c;
+            rb -= cbar * c * i2r;
+        }
         wo[0] += rb; wo[1] += ub; wo[2] += pb;
     };
     side(L, EL, cL, fLb, uLb, uLb_, cLb, wl);
@@ -160,11 +168,11 @@ k1d_adjoint_stage(const double* __restrict__ U, const double* __restrict__ Lout,
     // (rho, u, p) = prim(rho, m, E): transpose of its Jacobian at cell i
     int e = h + i;
     double rho = U[e], mom = U[nt + e], erg = U[2 * nt + e];
-    double u = mom / rho;
+    double u = mom / rho, ir = 1.0 / rho;
     double praw = gm1 * (erg - 0.5 * rho * u * u);
     double act = (praw < 0.0) ? 0.0 : 1.0;
-    double rb = wb[0] - wb[1] * u / rho + act * wb[2] * gm1 * 0.5 * u * u;
-    double mb = wb[1] / rho - act * wb[2] * gm1 * u;
+    double rb = wb[0] - wb[1] * u * ir + act * wb[2] * gm1 * 0.5 * u * u;
+    double mb = wb[1] * ir - act * wb[2] * gm1 * u;
     double Eb = act * wb[2] * gm1;
     double out[3] = { Lo[0][q + 1] + rb, Lo[1][q + 1] + mb, Lo[2][q + 1] + Eb };
     for (int k = 0; k < 3; ++k) {

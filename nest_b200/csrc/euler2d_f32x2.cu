@@ -308,15 +308,16 @@ __device__ __forceinline__ void x2_body(const StageArgs<float>& a, int strip, in
     }
 }
 
-// Register budgets of the plain (no repair) stage kernels.  ptxas left to
-// itself gives stage 2 128 registers with a small spill; a budget of 120
-// (17 warps per SM) measured 0.247 ms instead of 0.341 ms per launch at 4096^2
-// (B200, 16-row tiles, one warp per block); stage 1 sits at 117 either way.
+// Register budgets of the plain (no repair) stage kernels, from a sweep at
+// 4096^2 (B200, 16-row tiles, one warp per block): stage 2 under
+// __launch_bounds__(256) alone measured 0.341 ms per launch; with an explicit
+// budget of 120-128 it measured 0.243-0.247 ms, and 0.35 ms again at 118 and
+// below.  Stage 1 measured 0.218-0.220 ms for every budget from 116 to 128.
 #ifndef NEST_X2_REGS1
-#define NEST_X2_REGS1 120
+#define NEST_X2_REGS1 128
 #endif
 #ifndef NEST_X2_REGS2
-#define NEST_X2_REGS2 120
+#define NEST_X2_REGS2 124
 #endif
 
 __global__ void __maxnreg__(NEST_X2_REGS1) k2d_f32x2_1(StageArgs<float> a) {
