@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--adjoint2d-n", type=int, default=2048)
     ap.add_argument("--adjoint2d-steps", type=int, default=4000)
     ap.add_argument("--no-adjoint2d", action="store_true")
+    ap.add_argument("--extras", default="batched,adjoint1d,sod1d,adjoint2d",
+                    help="comma list of extra measurements to run (with extras on)")
     return ap.parse_args()
 
 
@@ -434,12 +436,17 @@ def run_ours(args, ws, rank, local):
         "gpu_launches": launches,
     }
     if not args.no_extras:
-        out["batched_kh"] = bench_batch(args, ws)
-        out["adjoint_1d"] = bench_adjoint(args)
-        out["sod_1d"] = bench_sod1d()
-        if not args.no_adjoint2d:
+        ex = {e.strip() for e in args.extras.split(",")}
+        if "batched" in ex:
+            out["batched_kh"] = bench_batch(args, ws)
+        if "adjoint1d" in ex:
+            out["adjoint_1d"] = bench_adjoint(args)
+        if "sod1d" in ex:
+            out["sod_1d"] = bench_sod1d()
+        if "adjoint2d" in ex and not args.no_adjoint2d:
             out["adjoint_2d_kh"] = bench_adjoint2d(args)
-        out["gpu_launches_extras"] = out["batched_kh"]["launches"] + out["adjoint_1d"]["launches"]
+        out["gpu_launches_extras"] = sum(out[k]["launches"] for k in ("batched_kh", "adjoint_1d", "sod_1d")
+                                         if k in out)
     if ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(n, args.cpu_seconds)
     return out
@@ -605,6 +612,8 @@ def bench_adjoint2d(args):
         s.close()
     g64, g32 = grads["f64"], grads["f32"]
     out["f32_vs_f64_grad_rel_l2"] = float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))
+    out["f32_vs_f64_grad_cosine"] = float(np.sum(g32 * g64) / (np.linalg.norm(g32) * np.linalg.norm(g64)))
+    out["grad_l2"] = {"f64": float(np.linalg.norm(g64)), "f32": float(np.linalg.norm(g32))}
     out.update({"n": n, "steps": K, "policy": "binomial (snapshots fitting 40 GB)",
                 "loss": "integral of 1/2 rho v^2 dA at t_end", "gradient": "d loss / d v(t=0)",
                 "launches": None})

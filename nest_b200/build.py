@@ -36,6 +36,7 @@ UNITS = {
     "adjoint.cpp": ["-x", "cu"],
     "exchange.cu": [],
     "adjoint2d.cu": [],
+    "adjoint2d_f32.cu": ["-use_fast_math"],
     "datio.cpp": ["-x", "cu", "-Xcompiler", "-ffp-contract=off"],
 }
 

@@ -13,14 +13,23 @@
 //   active argument of each Davis min / max), slope adjoints
 //   sbar = WLbar/2 (face above) - WRbar/2 (face below) per axis, minmod
 //   subgradients, Wbar gathered per cell, Ubar = Ubar' + (dW/dU)^T Wbar.
-// A CTA owns a 16 x 16 tile; every intermediate lives in shared memory.
+// A CTA of 256 threads owns a tile of ATX = 13 rows x ATY = 16 columns; every
+// intermediate lives in shared memory.  The tile shape makes both face sets
+// fit one pass of the CTA: (ATX + 3) x ATY = 256 x-faces and ATX x (ATY + 3)
+// = 247 y-faces, so every thread runs one x-face and one y-face reverse HLLE.
 #pragma once
 
 #include "euler2d_kernels.cuh"
 
 namespace nestb {
 
-constexpr int AT = 16;  // tile edge
+#ifndef NEST_ADJ_ATX
+#define NEST_ADJ_ATX 13
+#define NEST_ADJ_ATY 16
+#define NEST_ADJ_NT 256
+#endif
+constexpr int ATX = NEST_ADJ_ATX, ATY = NEST_ADJ_ATY;  // tile rows, tile columns
+constexpr int ANT = NEST_ADJ_NT;                       // threads per CTA
 
 template <typename T>
 struct Adj4 { T r, n, t, p; };
@@ -28,9 +37,10 @@ struct Adj4 { T r, n, t, p; };
 // Reverse sweep of hlle4 (normal n, transverse t) for one face.
 template <typename T>
 __device__ __forceinline__ void hlle4_adj(T gamma, T gm1, Adj4<T> L, Adj4<T> R, const T fb[4], T wl[4], T wr[4]) {
+    const T igm1 = T(1) / gm1;
     T cL = sqrt(gamma * L.p / L.r), cR = sqrt(gamma * R.p / R.r);
-    T EL = L.p / gm1 + T(0.5) * L.r * (L.n * L.n + L.t * L.t);
-    T ER = R.p / gm1 + T(0.5) * R.r * (R.n * R.n + R.t * R.t);
+    T EL = L.p * igm1 + T(0.5) * L.r * (L.n * L.n + L.t * L.t);
+    T ER = R.p * igm1 + T(0.5) * R.r * (R.n * R.n + R.t * R.t);
     T aL = L.n - cL, aR = R.n - cR, bL = L.n + cL, bR = R.n + cR;
     T SL = smin(aL, aR), SR = smax(bL, bR);
     bool slR = aR < aL, srR = bL < bR;
@@ -44,16 +54,17 @@ __device__ __forceinline__ void hlle4_adj(T gamma, T gm1, Adj4<T> L, Adj4<T> R, 
     } else if (SR <= T(0)) {
         for (int k = 0; k < 4; ++k) fRb[k] = fb[k];
     } else {
-        T D = SR - SL, iD = T(1) / D;
+        const T iD = T(1) / (SR - SL);
         for (int k = 0; k < 4; ++k) {
             T dU = UR[k] - UL[k];
             T F = (SR * FL[k] - SL * FR[k] + SL * SR * dU) * iD;
-            fLb[k] = fb[k] * SR * iD;
-            fRb[k] = -fb[k] * SL * iD;
-            uRb[k] = fb[k] * SL * SR * iD;
+            T gk = fb[k] * iD;
+            fLb[k] = gk * SR;
+            fRb[k] = -gk * SL;
+            uRb[k] = gk * SL * SR;
             uLb[k] = -uRb[k];
-            SLb += fb[k] * (-FR[k] + SR * dU + F) * iD;
-            SRb += fb[k] * (FL[k] + SL * dU - F) * iD;
+            SLb += gk * (-FR[k] + SR * dU + F);
+            SRb += gk * (FL[k] + SL * dU - F);
         }
     }
     T nLb = 0, nRb = 0, cLb = 0, cRb = 0;
@@ -67,8 +78,12 @@ __device__ __forceinline__ void hlle4_adj(T gamma, T gm1, Adj4<T> L, Adj4<T> R, 
         Eb += fb_[3] * S.n; pb += fb_[3] * S.n; nb += fb_[3] * (E + S.p);         // (E + p) n
         rb += ub_[0]; rb += ub_[1] * S.n; nb += ub_[1] * S.r;
         rb += ub_[2] * S.t; tb += ub_[2] * S.r; Eb += ub_[3];
-        pb += Eb / gm1; rb += Eb * T(0.5) * (S.n * S.n + S.t * S.t); nb += Eb * S.r * S.n; tb += Eb * S.r * S.t;
-        if (c > T(0)) { pb += cb * gamma / (T(2) * S.r * c); rb -= cb * c / (T(2) * S.r); }
+        pb += Eb * igm1; rb += Eb * T(0.5) * (S.n * S.n + S.t * S.t); nb += Eb * S.r * S.n; tb += Eb * S.r * S.t;
+        if (c > T(0)) {  // c = sqrt(g p / r): dc/dp = g / (2 r c), dc/dr = -c / (2 r)
+            const T i2r = T(0.5) / S.r;
+            pb += cb * gamma * i2r / c;
+            rb -= cb * c * i2r;
+        }
         wo[0] += rb; wo[1] += nb; wo[2] += tb; wo[3] += pb;
     };
     side(L, EL, cL, fLb, uLb, nLb, cLb, wl);
@@ -86,14 +101,14 @@ __device__ __forceinline__ T mmslope(T d1, T d2, signed char& br) {
 // Shared-memory image of one tile.
 template <typename T>
 struct AdjSmem {
-    static constexpr int E3 = AT + 6, E2 = AT + 4;
-    T W[4][E3][E3];              // primitives of cells (i0-3 .., j0-3 ..)
-    T Lo[4][E2][E2];             // output adjoint of cells (i0-2 .., j0-2 ..), alpha applied
-    T Sx[4][E2][AT];             // x slopes of rows i0-2 .. under the tile columns
-    T Sy[4][AT][E2];             // y slopes of columns j0-2 .. in the tile rows
-    T XL[4][AT + 3][AT], XR[4][AT + 3][AT];  // x-face state adjoints, faces between rows i0-2+f, i0-1+f
-    T YL[4][AT][AT + 3], YR[4][AT][AT + 3];  // y-face state adjoints
-    signed char Bx[4][E2][AT], By[4][AT][E2];  // minmod branch: 0 none, 1 first, 2 second difference
+    static constexpr int RX3 = ATX + 6, RY3 = ATY + 6, RX2 = ATX + 4, RY2 = ATY + 4;
+    T W[4][RX3][RY3];                // primitives of cells (i0-3 .., j0-3 ..)
+    T Lo[4][RX2][RY2];               // output adjoint of cells (i0-2 .., j0-2 ..), alpha applied
+    T Sx[4][RX2][ATY];               // x slopes of rows i0-2 .. under the tile columns
+    T Sy[4][ATX][RY2];               // y slopes of columns j0-2 .. in the tile rows
+    T XL[4][ATX + 3][ATY], XR[4][ATX + 3][ATY];  // x-face state adjoints, faces between rows i0-2+f, i0-1+f
+    T YL[4][ATX][ATY + 3], YR[4][ATX][ATY + 3];  // y-face state adjoints, faces between columns j0-2+f, j0-1+f
+    signed char Bx[4][RX2][ATY], By[4][ATX][RY2];  // minmod branch: 0 none, 1 first, 2 second difference
 };
 
 // Lin = alpha * adj(U, Lout) + beta * Extra.  All arrays use the solver's
@@ -102,7 +117,8 @@ struct AdjSmem {
 template <typename T>
 __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lout, const T* __restrict__ Extra,
                                T* __restrict__ Lin, const Geo2D& g, T lx, T ly, T alpha, T beta) {
-    constexpr int E3 = AT + 6, E2 = AT + 4;
+    constexpr int RX3 = ATX + 6, RY3 = ATY + 6, RX2 = ATX + 4, RY2 = ATY + 4;
+    static_assert((ATX + 3) * ATY <= ANT && ATX * (ATY + 3) <= ANT, "one face of each kind per thread");
     extern __shared__ __align__(16) unsigned char adj_smem_raw[];
     AdjSmem<T>& S = *reinterpret_cast<AdjSmem<T>*>(adj_smem_raw);
     auto& W = S.W;
@@ -116,75 +132,89 @@ __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lo
     auto& YL = S.YL;
     auto& YR = S.YR;
     const int tid = threadIdx.x;
-    const int i0 = blockIdx.y * AT, j0 = blockIdx.x * AT;
+    const int i0 = blockIdx.y * ATX, j0 = blockIdx.x * ATY;
     const long long vs = g.vstride;
     const T gamma = (T)g.gamma, gm1 = (T)(g.gamma - 1.0);
     // periodic wrap; tile cells beyond the domain (only read by threads that
     // return early) may lie more than one period away on small domains
-    auto wrapi = [&](int i) { int r = i % g.nx; return r < 0 ? r + g.nx : r; };
-    auto wrapj = [&](int j) { int r = j % g.ny; return r < 0 ? r + g.ny : r; };
-    for (int t = tid; t < E3 * E3; t += AT * AT) {
-        int a = t / E3, b = t % E3;
+    auto wrapi = [&](int i) {
+        if ((unsigned)i < (unsigned)g.nx) return i;
+        int r = i % g.nx;
+        return r < 0 ? r + g.nx : r;
+    };
+    auto wrapj = [&](int j) {
+        if ((unsigned)j < (unsigned)g.ny) return j;
+        int r = j % g.ny;
+        return r < 0 ? r + g.ny : r;
+    };
+    for (int t = tid; t < RX3 * RY3; t += ANT) {
+        int a = t / RY3, b = t % RY3;
         long long o = g.at(wrapi(i0 - 3 + a), wrapj(j0 - 3 + b));
         Prim4<T> w = cons2prim<T, false>(U[o], U[vs + o], U[2 * vs + o], U[3 * vs + o], gm1);
         W[0][a][b] = w.r; W[1][a][b] = w.u; W[2][a][b] = w.v; W[3][a][b] = w.p;
     }
-    for (int t = tid; t < E2 * E2; t += AT * AT) {
-        int a = t / E2, b = t % E2;
+    for (int t = tid; t < RX2 * RY2; t += ANT) {
+        int a = t / RY2, b = t % RY2;
         long long o = g.at(wrapi(i0 - 2 + a), wrapj(j0 - 2 + b));
         for (int k = 0; k < 4; ++k) Lo[k][a][b] = alpha * Lout[k * vs + o];
     }
     __syncthreads();
-    // slopes: x for rows i0-2 .. i0+AT+1 (index a) under the tile columns, y mirrored
-    for (int t = tid; t < E2 * AT; t += AT * AT) {
-        int a = t / AT, b = t % AT;
+    // x slopes of rows i0-2 .. i0+ATX+1 (index a) under the tile columns
+    for (int t = tid; t < RX2 * ATY; t += ANT) {
+        int a = t / ATY, b = t % ATY;
         for (int k = 0; k < 4; ++k) {
             signed char br;
             Sx[k][a][b] = mmslope(W[k][a + 1][b + 3] - W[k][a][b + 3], W[k][a + 2][b + 3] - W[k][a + 1][b + 3], br);
             Bx[k][a][b] = br;
-            Sy[k][b][a] = mmslope(W[k][b + 3][a + 1] - W[k][b + 3][a], W[k][b + 3][a + 2] - W[k][b + 3][a + 1], br);
-            By[k][b][a] = br;
+        }
+    }
+    // y slopes of columns j0-2 .. j0+ATY+1 (index c) in the tile rows
+    for (int t = tid; t < ATX * RY2; t += ANT) {
+        int a = t / RY2, c = t % RY2;
+        for (int k = 0; k < 4; ++k) {
+            signed char br;
+            Sy[k][a][c] = mmslope(W[k][a + 3][c + 1] - W[k][a + 3][c], W[k][a + 3][c + 2] - W[k][a + 3][c + 1], br);
+            By[k][a][c] = br;
         }
     }
     __syncthreads();
-    // face adjoints: x faces f between rows a = i0-2+f and a+1 (Sx index f, f+1; Lo row f, f+1)
-    for (int t = tid; t < (AT + 3) * AT; t += AT * AT) {
-        int f = t / AT, b = t % AT;
-        {
-            Adj4<T> L = { W[0][f + 1][b + 3] + T(0.5) * Sx[0][f][b], W[1][f + 1][b + 3] + T(0.5) * Sx[1][f][b],
-                          W[2][f + 1][b + 3] + T(0.5) * Sx[2][f][b], W[3][f + 1][b + 3] + T(0.5) * Sx[3][f][b] };
-            Adj4<T> R = { W[0][f + 2][b + 3] - T(0.5) * Sx[0][f + 1][b], W[1][f + 2][b + 3] - T(0.5) * Sx[1][f + 1][b],
-                          W[2][f + 2][b + 3] - T(0.5) * Sx[2][f + 1][b], W[3][f + 2][b + 3] - T(0.5) * Sx[3][f + 1][b] };
-            T fb[4], wl[4] = {0, 0, 0, 0}, wr[4] = {0, 0, 0, 0};
-            for (int k = 0; k < 4; ++k) fb[k] = lx * (Lo[k][f + 1][b + 2] - Lo[k][f][b + 2]);
-            // components (rho, mu, mv, E) -> (rho, normal, transverse, E): x normal = u
-            hlle4_adj(gamma, gm1, L, R, fb, wl, wr);
-            for (int k = 0; k < 4; ++k) { XL[k][f][b] = wl[k]; XR[k][f][b] = wr[k]; }
-        }
-        {
-            // y faces between columns c = j0-2+f and c+1 under tile row b
-            Adj4<T> L = { W[0][b + 3][f + 1] + T(0.5) * Sy[0][b][f], W[2][b + 3][f + 1] + T(0.5) * Sy[2][b][f],
-                          W[1][b + 3][f + 1] + T(0.5) * Sy[1][b][f], W[3][b + 3][f + 1] + T(0.5) * Sy[3][b][f] };
-            Adj4<T> R = { W[0][b + 3][f + 2] - T(0.5) * Sy[0][b][f + 1], W[2][b + 3][f + 2] - T(0.5) * Sy[2][b][f + 1],
-                          W[1][b + 3][f + 2] - T(0.5) * Sy[1][b][f + 1], W[3][b + 3][f + 2] - T(0.5) * Sy[3][b][f + 1] };
-            // flux order (rho, normal = mv, transverse = mu, E)
-            T fb[4] = { ly * (Lo[0][b + 2][f + 1] - Lo[0][b + 2][f]), ly * (Lo[2][b + 2][f + 1] - Lo[2][b + 2][f]),
-                        ly * (Lo[1][b + 2][f + 1] - Lo[1][b + 2][f]), ly * (Lo[3][b + 2][f + 1] - Lo[3][b + 2][f]) };
-            T wl[4] = {0, 0, 0, 0}, wr[4] = {0, 0, 0, 0};
-            hlle4_adj(gamma, gm1, L, R, fb, wl, wr);
-            // back to (rho, u, v, p)
-            YL[0][b][f] = wl[0]; YL[1][b][f] = wl[2]; YL[2][b][f] = wl[1]; YL[3][b][f] = wl[3];
-            YR[0][b][f] = wr[0]; YR[1][b][f] = wr[2]; YR[2][b][f] = wr[1]; YR[3][b][f] = wr[3];
-        }
+    if (tid < (ATX + 3) * ATY) {
+        // x face f between rows i0-2+f and i0-1+f under tile column b (Sx index f, f+1; Lo row f, f+1)
+        const int f = tid / ATY, b = tid % ATY;
+        Adj4<T> L = { W[0][f + 1][b + 3] + T(0.5) * Sx[0][f][b], W[1][f + 1][b + 3] + T(0.5) * Sx[1][f][b],
+                      W[2][f + 1][b + 3] + T(0.5) * Sx[2][f][b], W[3][f + 1][b + 3] + T(0.5) * Sx[3][f][b] };
+        Adj4<T> R = { W[0][f + 2][b + 3] - T(0.5) * Sx[0][f + 1][b], W[1][f + 2][b + 3] - T(0.5) * Sx[1][f + 1][b],
+                      W[2][f + 2][b + 3] - T(0.5) * Sx[2][f + 1][b], W[3][f + 2][b + 3] - T(0.5) * Sx[3][f + 1][b] };
+        T fb[4], wl[4] = {0, 0, 0, 0}, wr[4] = {0, 0, 0, 0};
+        for (int k = 0; k < 4; ++k) fb[k] = lx * (Lo[k][f + 1][b + 2] - Lo[k][f][b + 2]);
+        // components (rho, mu, mv, E) -> (rho, normal, transverse, E): x normal = u
+        hlle4_adj(gamma, gm1, L, R, fb, wl, wr);
+        for (int k = 0; k < 4; ++k) { XL[k][f][b] = wl[k]; XR[k][f][b] = wr[k]; }
+    }
+    if (tid < ATX * (ATY + 3)) {
+        // y face f between columns j0-2+f and j0-1+f in tile row a
+        const int a = tid / (ATY + 3), f = tid % (ATY + 3);
+        Adj4<T> L = { W[0][a + 3][f + 1] + T(0.5) * Sy[0][a][f], W[2][a + 3][f + 1] + T(0.5) * Sy[2][a][f],
+                      W[1][a + 3][f + 1] + T(0.5) * Sy[1][a][f], W[3][a + 3][f + 1] + T(0.5) * Sy[3][a][f] };
+        Adj4<T> R = { W[0][a + 3][f + 2] - T(0.5) * Sy[0][a][f + 1], W[2][a + 3][f + 2] - T(0.5) * Sy[2][a][f + 1],
+                      W[1][a + 3][f + 2] - T(0.5) * Sy[1][a][f + 1], W[3][a + 3][f + 2] - T(0.5) * Sy[3][a][f + 1] };
+        // flux order (rho, normal = mv, transverse = mu, E)
+        T fb[4] = { ly * (Lo[0][a + 2][f + 1] - Lo[0][a + 2][f]), ly * (Lo[2][a + 2][f + 1] - Lo[2][a + 2][f]),
+                    ly * (Lo[1][a + 2][f + 1] - Lo[1][a + 2][f]), ly * (Lo[3][a + 2][f + 1] - Lo[3][a + 2][f]) };
+        T wl[4] = {0, 0, 0, 0}, wr[4] = {0, 0, 0, 0};
+        hlle4_adj(gamma, gm1, L, R, fb, wl, wr);
+        // back to (rho, u, v, p)
+        YL[0][a][f] = wl[0]; YL[1][a][f] = wl[2]; YL[2][a][f] = wl[1]; YL[3][a][f] = wl[3];
+        YR[0][a][f] = wr[0]; YR[1][a][f] = wr[2]; YR[2][a][f] = wr[1]; YR[3][a][f] = wr[3];
     }
     __syncthreads();
-    // gather for tile cell (a, b): x faces a+1 (below, WR) and a+2 (above, WL);
-    // slope adjoint of row r (Sx index r+... ) = XL(face r+1... ) see indices below
-    const int a = tid / AT, b = tid % AT;
+    if (tid >= ATX * ATY) return;
+    const int a = tid / ATY, b = tid % ATY;
     const int i = i0 + a, j = j0 + b;
     if (i >= g.nx || j >= g.ny) return;
-    // Sx/Bx index of row i0-2+q is q; cell row i is q = a+2.  Face f lies between
+    // Sx/Bx index of row i0-2+q is q; cell row i is q = a+2.  x face f lies between
     // rows i0-2+f and i0-1+f, so cell row i0-2+q has lower face q-1 and upper face q.
+    // Columns likewise with r = b+2.
     auto sbx = [&](int k, int q) { return T(0.5) * XL[k][q][b] - T(0.5) * XR[k][q - 1][b]; };
     auto sby = [&](int k, int q) { return T(0.5) * YL[k][a][q] - T(0.5) * YR[k][a][q - 1]; };
     T wb[4];
@@ -203,13 +233,14 @@ __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lo
     }
     const long long o = g.at(i, j);
     T rho = U[o], mu = U[vs + o], mv = U[2 * vs + o], E = U[3 * vs + o];
+    const T ir = T(1) / rho;
     T u = mu / rho, v = mv / rho;
     T praw = gm1 * (E - (T(0.5) * rho * u * u + T(0.5) * rho * v * v));
     T act = (praw < T(0)) ? T(0) : T(1);
     T q2 = T(0.5) * (u * u + v * v);
-    T rb = wb[0] - wb[1] * u / rho - wb[2] * v / rho + act * wb[3] * gm1 * q2;
-    T mub = wb[1] / rho - act * wb[3] * gm1 * u;
-    T mvb = wb[2] / rho - act * wb[3] * gm1 * v;
+    T rb = wb[0] - (wb[1] * u + wb[2] * v) * ir + act * wb[3] * gm1 * q2;
+    T mub = wb[1] * ir - act * wb[3] * gm1 * u;
+    T mvb = wb[2] * ir - act * wb[3] * gm1 * v;
     T Eb = act * wb[3] * gm1;
     T out[4] = { Lo[0][a + 2][b + 2] + rb, Lo[1][a + 2][b + 2] + mub, Lo[2][a + 2][b + 2] + mvb, Lo[3][a + 2][b + 2] + Eb };
     for (int k = 0; k < 4; ++k) {
