@@ -498,7 +498,7 @@ def bench_batch(args, ws):
             "hbm_gbs_equiv_per_gpu": value / ws * 40 / 1e9, "sim_time_range": [float(times.min()), float(times.max())],
             "fp64_totals_rel_drift": {"mass": float(drift[0]), "energy": float(drift[3])},
             "tiling": {"rows_per_item": tiling[0], "warps_per_block": tiling[1], "blocks_per_sm": tiling[2]},
-            "launches": 2 * args.batch_steps, "dtype": "f32 (FP64 totals, time, repair)"}
+            "launches": 4 * args.batch_steps, "dtype": "f32 (FP64 totals, time, repair)"}
 
 
 def bench_adjoint(args):

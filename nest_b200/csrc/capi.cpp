@@ -11,6 +11,7 @@
 // src/backend_cuda/euler1d_solver.cu:159-235) on top of a 1D FP64 solver.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -760,6 +761,10 @@ BatchArgs<T> batch_args(nest_batch* b, const LoopParams& lp, int p) {
     BatchArgs<T> a;
     a.U = (T*)b->U; a.U1 = (T*)b->U1; a.probs = b->dprobs; a.items = b->ditems; a.nitems = (int)b->items.size();
     a.ctrls = b->ctrls; a.partials = b->partials; a.lp = lp; a.p = p; a.tx = b->tx;
+    a.nprobs = b->count;
+    int ring = 0;
+    for (const BatchProblem& q : b->probs) ring = std::max(ring, 4 * (q.g.nx + q.g.ny));
+    a.ghost_blocks = std::min(32, (ring + 255) / 256);
     return a;
 }
 

@@ -11,8 +11,9 @@
 //   * x-faces: one packed HLLE for the faces under columns a and b,
 //   * y-faces: one packed HLLE for the faces a|b and b|a' (a' = next lane's
 //     first column), with 2 + 1 + 1 shuffles per variable.
-// Minmod is median(0, a, b) = max(min(a, b), min(max(a, b), 0)), which equals
-// nest's minmod (euler1d.hpp:112-115) without a multiply or branch.
+// Minmod takes three ALU operations (min.xorsign.abs, max, copysign) and the
+// HLLE flux is written in relative-flux form with dt/dx folded into its
+// weights (hlle2 below).
 // Compiled with -use_fast_math: reciprocal and rsqrt are single MUFU ops.
 #include "euler2d_kernels.cuh"
 #include "kernels.h"
@@ -22,24 +23,47 @@ namespace {
 
 constexpr int STRIP2 = 60;  // output columns per warp
 
+
 using F2 = float2;
 
 __device__ __forceinline__ F2 sp(float a) { return make_float2(a, a); }
 __device__ __forceinline__ F2 add2(F2 a, F2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ F2 sub2(F2 a, F2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ F2 sub2(F2 a, F2 b) {
+    F2 o;
+    asm("{\n\t.reg .b64 ta, tb, tr;\n\tmov.b64 ta, {%2, %3};\n\tmov.b64 tb, {%4, %5};\n\t"
+        "sub.rn.f32x2 tr, ta, tb;\n\tmov.b64 {%0, %1}, tr;\n\t}"
+        : "=f"(o.x), "=f"(o.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return o;
+}
 __device__ __forceinline__ F2 mul2(F2 a, F2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ F2 rcp2(F2 a) { return make_float2(__fdividef(1.f, a.x), __fdividef(1.f, a.y)); }
 __device__ __forceinline__ F2 rsq2(F2 a) { return make_float2(rsqrtf(a.x), rsqrtf(a.y)); }
 __device__ __forceinline__ F2 max2(F2 a, float b) { return make_float2(fmaxf(a.x, b), fmaxf(a.y, b)); }
-__device__ __forceinline__ F2 min2(F2 a, float b) { return make_float2(fminf(a.x, b), fminf(a.y, b)); }
-__device__ __forceinline__ F2 vmax2(F2 a, F2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
-__device__ __forceinline__ F2 vmin2(F2 a, F2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
 
-__device__ __forceinline__ float mm(float a, float b) { return fmaxf(fminf(a, b), fminf(fmaxf(a, b), 0.f)); }
+// nest's minmod (euler1d.hpp:112-115) in three ALU operations:
+// min.xorsign.abs gives min(|a|, |b|) carrying the sign sign(a) xor sign(b),
+// negative exactly when the signs differ; max(., 0) zeroes that case and
+// copysign restores sign(a).  Only the sign of a zero result can differ.
+__device__ __forceinline__ float mm(float a, float b) {
+    float t;
+    asm("min.xorsign.abs.f32 %0, %1, %2;" : "=f"(t) : "f"(a), "f"(b));
+    return copysignf(fmaxf(t, 0.f), a);
+}
 __device__ __forceinline__ F2 mm2(F2 a, F2 b) { return make_float2(mm(a.x, b.x), mm(a.y, b.y)); }
 
+// Three-input max (sm_100).
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float t;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(t) : "f"(a), "f"(b), "f"(c));
+    return t;
+}
+
 struct Q4 { F2 a, b, c, d; };  // four variables, each a column pair
+
+__device__ __forceinline__ Q4 q_fma(F2 h, const Q4& s, const Q4& w) {
+    return { fma2(h, s.a, w.a), fma2(h, s.b, w.b), fma2(h, s.c, w.c), fma2(h, s.d, w.d) };
+}
 
 // cons -> prim on a pair: (rho, mu, mv, E) -> (rho, u, v, p), p >= 0.
 template <bool REPAIR>
@@ -63,30 +87,35 @@ __device__ __forceinline__ Q4 prim2(const Q4& U, float gm1) {
     return w;
 }
 
-// Packed four-variable HLLE along the normal (states (rho, un, ut, p)),
-// branchless form of euler1d.hpp:178-242 with Davis speeds.
-__device__ __forceinline__ void hlle2(float gamma, float igm1,
+// Packed four-variable HLLE along the normal (states (rho, un, ut, p)) with
+// Davis speeds, euler1d.hpp:178-242, returning the flux times `scale`.
+// Written in relative-flux form: with sl = min(S_L, 0), sr = max(S_R, 0),
+//   F = [sr (F_L - sl U_L) - sl (F_R - sr U_R)] / (sr - sl),
+// which is the HLLE average in the subsonic case and reduces to F_L
+// (sl = 0) or F_R (sr = 0) in the supersonic ones, and
+//   F - s U = (q, q un + p, q ut, (un - s) E + p un),  q = rho (un - s).
+__device__ __forceinline__ void hlle2(float gamma, float igm1, F2 scale,
                                       F2 rL, F2 nL, F2 tL, F2 pL, F2 rR, F2 nR, F2 tR, F2 pR,
                                       F2& f0, F2& f1, F2& f2, F2& f3) {
     F2 g = sp(gamma), h = sp(0.5f);
     F2 gpL = mul2(g, pL), gpR = mul2(g, pR);
     F2 cL = mul2(gpL, rsq2(max2(mul2(gpL, rL), 1e-37f)));
     F2 cR = mul2(gpR, rsq2(max2(mul2(gpR, rR), 1e-37f)));
+    // nsl = -min(S_L, 0) = max(c_L - u_L, c_R - u_R, 0), sr = max(S_R, 0)
+    F2 aL = sub2(cL, nL), aR = sub2(cR, nR), bL = add2(nL, cL), bR = add2(nR, cR);
+    F2 nsl = make_float2(max3f(aL.x, aR.x, 0.f), max3f(aL.y, aR.y, 0.f));
+    F2 sr = make_float2(max3f(bL.x, bR.x, 0.f), max3f(bL.y, bR.y, 0.f));
+    F2 inv = mul2(scale, rcp2(max2(add2(sr, nsl), 1e-30f)));
+    F2 A = mul2(sr, inv);   //  scale sr / (sr - sl)
+    F2 B = mul2(nsl, inv);  // -scale sl / (sr - sl)
+    F2 dL = add2(nL, nsl), dR = sub2(nR, sr);
+    F2 qL = mul2(rL, dL), qR = mul2(rR, dR);
     F2 EL = fma2(pL, sp(igm1), mul2(mul2(h, rL), fma2(tL, tL, mul2(nL, nL))));
     F2 ER = fma2(pR, sp(igm1), mul2(mul2(h, rR), fma2(tR, tR, mul2(nR, nR))));
-    F2 SL = vmin2(sub2(nL, cL), sub2(nR, cR));
-    F2 SR = vmax2(add2(nL, cL), add2(nR, cR));
-    F2 mL = mul2(rL, nL), mR = mul2(rR, nR);
-    F2 sl = min2(SL, 0.f), sr = max2(SR, 0.f);
-    F2 inv = rcp2(max2(sub2(sr, sl), 1e-30f));
-    F2 A = mul2(sr, inv);
-    F2 B = mul2(make_float2(-sl.x, -sl.y), inv);  // -sl / (sr - sl)
-    F2 Cc = mul2(mul2(sl, sr), inv);
-    // f = A FL + B FR + Cc (UR - UL)
-    f0 = fma2(Cc, sub2(rR, rL), fma2(A, mL, mul2(B, mR)));
-    f1 = fma2(Cc, sub2(mR, mL), fma2(A, fma2(mL, nL, pL), mul2(B, fma2(mR, nR, pR))));
-    f2 = fma2(Cc, sub2(mul2(rR, tR), mul2(rL, tL)), fma2(A, mul2(mL, tL), mul2(B, mul2(mR, tR))));
-    f3 = fma2(Cc, sub2(ER, EL), fma2(A, mul2(add2(EL, pL), nL), mul2(B, mul2(add2(ER, pR), nR))));
+    f0 = fma2(A, qL, mul2(B, qR));
+    f1 = fma2(A, fma2(qL, nL, pL), mul2(B, fma2(qR, nR, pR)));
+    f2 = fma2(A, mul2(qL, tL), mul2(B, mul2(qR, tR)));
+    f3 = fma2(A, fma2(dL, EL, mul2(pL, nL)), mul2(B, fma2(dR, ER, mul2(pR, nR))));
 }
 
 __device__ __forceinline__ Q4 minmod_pair(const Q4& m, const Q4& o, const Q4& p) {
@@ -105,8 +134,15 @@ __device__ __forceinline__ F2 yslope(F2 w) {
 
 // One warp's work: the rows of tile `tile_row` under column strip `strip`.
 // The warp owning strip 0 / tile 0 publishes the step's dt for the domain.
-template <int STAGE, bool REPAIR>
-__device__ __forceinline__ void x2_body(const StageArgs<float>& a, int strip, int tile_row) {
+//
+// Row march: before the loop the window holds the primitives of rows q and
+// q+1, the upper x-face state P of row q and the x-flux of face q-1/2 (all
+// for q = the tile's first row); iteration q adds row q+2, computes the
+// x-flux of face q+1/2 and the y-fluxes of row q, and updates row q.  Fluxes
+// come out of hlle2 already multiplied by dt/dx (dt/dy), and by 1/2 in stage
+// 2, where the Heun average is folded into the update.
+template <int STAGE, bool REPAIR, bool TOT, bool GHOST, class A>
+__device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
     const Geo2D& g = a.g;
     const int lane = threadIdx.x & 31;
     const float gamma = (float)g.gamma;
@@ -130,165 +166,204 @@ __device__ __forceinline__ void x2_body(const StageArgs<float>& a, int strip, in
         if (!a.ctrl->active[a.p]) return;
         dt = a.ctrl->dt[a.p];
     }
-    const float dtdx = (float)(dt / g.dx);
-    const float dtdy = (float)(dt / g.dy);
+    const double hs = STAGE == 2 ? 0.5 : 1.0;
+    const float dtdx = (float)(hs * dt / g.dx);
+    const float dtdy = (float)(hs * dt / g.dy);
+    const F2 sx = sp(dtdx), sy_ = sp(dtdy);
 
+    // geometry used inside the row loop, held in registers (in the batched
+    // kernel `g` lives in global memory)
+    const int nx = g.nx, ny = g.ny, pitch = g.pitch;
     const int j0 = strip * STRIP2;
-    if (j0 >= g.ny) return;  // whole warp idle
+    if (j0 >= ny) return;  // whole warp idle
     const int ca = j0 - 2 + 2 * lane;  // first of the lane's two columns
     // element offset of the pair within a row; pairs past the ghost ring read
     // the row padding (finite, discarded)
-    const int coff = min(ca + 2, g.pitch - 2);
+    const int coff = min(ca + 2, pitch - 2);
     const bool lane_out = lane >= 1 && lane <= 30;
-    const bool out_a = lane_out && ca < g.ny;
-    const bool out_b = lane_out && ca + 1 < g.ny;
+    const bool out_a = lane_out && ca < ny;
+    const bool out_b = lane_out && ca + 1 < ny;
+    const bool edge_col = ca < 2 || ca + 1 >= ny - 2;
     const int i0 = tile_row * a.tx;
-    if (i0 >= g.nx) return;
-    const int rows = min(a.tx, g.nx - i0);
+    if (i0 >= nx) return;
+    const int rows = min(a.tx, nx - i0);
+    const int last_row = nx + 1;  // last ghost row: loads past it are clamped to it
     const long long vs = g.vstride;
     const float* __restrict__ Ui = a.Uin;
+    const float* Unp = a.Un;
 
     auto load = [&](int i, Q4& q) {
-        const long long o = (long long)(i + 2) * g.pitch + coff;
+        const long long o = (long long)(min(i, last_row) + 2) * pitch + coff;
         q.a = __ldg(reinterpret_cast<const F2*>(Ui + o));
         q.b = __ldg(reinterpret_cast<const F2*>(Ui + vs + o));
         q.c = __ldg(reinterpret_cast<const F2*>(Ui + 2 * vs + o));
         q.d = __ldg(reinterpret_cast<const F2*>(Ui + 3 * vs + o));
     };
-
-    // Window entering iteration r: W0 = W(r-2), W1 = W(r-1) (primitives),
-    // P0 = W(r-2) + S(r-2)/2 (upper x-face state of row r-2), Fp = x-flux of
-    // face r-5/2.  The conserved values of the row being updated are re-read
-    // from L1 (they were loaded two iterations earlier); stage 2's U^n row is
-    // requested at the top of the iteration, ahead of the flux work.
-    Q4 W0, W1, P0, Fp, nxt, un;
-    float smx = 0.f, smy = 0.f;
-    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
-    const F2 half = sp(0.5f), mhalf = sp(-0.5f);
-    const float* Unp = a.Un;
     auto load_un = [&](int i, Q4& q) {
-        const long long o = (long long)(i + 2) * g.pitch + coff;
+        const long long o = (long long)(i + 2) * pitch + coff;
         q.a = *reinterpret_cast<const F2*>(Unp + o);
         q.b = *reinterpret_cast<const F2*>(Unp + vs + o);
         q.c = *reinterpret_cast<const F2*>(Unp + 2 * vs + o);
         q.d = *reinterpret_cast<const F2*>(Unp + 3 * vs + o);
     };
+    auto prefetch_un = [&](int i) {
+        const float* q = Unp + (long long)(i + 2) * pitch + coff;
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(q + vs));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(q + 2 * vs));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(q + 3 * vs));
+    };
+    const F2 half = sp(0.5f), mhalf = sp(-0.5f);
 
-    load(i0 - 2, nxt);
-    for (int r = -2; r <= rows + 1; ++r) {
+    // prologue: rows i0-2 .. i0+1, x-flux of face i0-1/2
+    Q4 Wq, Wq1, Pq, Fm, nxt;
+    {
+        Q4 c0, c1, c2, c3;
+        load(i0 - 2, c0); load(i0 - 1, c1); load(i0, c2); load(i0 + 1, c3);
+        load(i0 + 2, nxt);
+        Q4 Wa = prim2<REPAIR>(c0, gm1), Wb = prim2<REPAIR>(c1, gm1);
+        Wq = prim2<REPAIR>(c2, gm1); Wq1 = prim2<REPAIR>(c3, gm1);
+        Q4 Sb = minmod_pair(Wa, Wb, Wq), Sq = minmod_pair(Wb, Wq, Wq1);
+        Q4 Pb = q_fma(half, Sb, Wb), Mq = q_fma(mhalf, Sq, Wq);
+        hlle2(gamma, igm1, sx, Pb.a, Pb.b, Pb.c, Pb.d, Mq.a, Mq.b, Mq.c, Mq.d, Fm.a, Fm.b, Fm.c, Fm.d);
+        Pq = q_fma(half, Sq, Wq);
+    }
+
+    if (STAGE == 2) prefetch_un(i0);
+    float smx = 0.f, smy = 0.f;
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < rows; ++k) {
+        const int i = i0 + k;
         Q4 cur = nxt;
-        if (r + 1 <= rows + 1) load(i0 + r + 1, nxt);
-        Q4 C0;
-        if (r >= 2) {
-            load(i0 + r - 2, C0);  // L1 hit: loaded as `cur` two iterations ago
-            if (STAGE == 2) load_un(i0 + r - 2, un);  // used after this iteration's flux work
-        }
+        load(i + 3, nxt);
+        // stage 2: U^n of the next row is pulled into L1 one iteration ahead
+        // and loaded after the flux work, so it holds no registers meanwhile
+        if (STAGE == 2 && k + 1 < rows) prefetch_un(i + 1);
+
+        // x-face i+1/2 from rows i .. i+2
         Q4 W2 = prim2<REPAIR>(cur, gm1);
-        Q4 P1, M1;
-        if (r >= 0) {
-            Q4 S1 = minmod_pair(W0, W1, W2);  // x-slope of row r-1
-            P1 = { fma2(half, S1.a, W1.a), fma2(half, S1.b, W1.b), fma2(half, S1.c, W1.c), fma2(half, S1.d, W1.d) };
-            M1 = { fma2(mhalf, S1.a, W1.a), fma2(mhalf, S1.b, W1.b), fma2(mhalf, S1.c, W1.c), fma2(mhalf, S1.d, W1.d) };
+        Q4 S1 = minmod_pair(Wq, Wq1, W2);
+        Q4 M1 = q_fma(mhalf, S1, Wq1);
+        Q4 Fc;
+        hlle2(gamma, igm1, sx, Pq.a, Pq.b, Pq.c, Pq.d, M1.a, M1.b, M1.c, M1.d, Fc.a, Fc.b, Fc.c, Fc.d);
+
+        // The conserved values of row i (an L1 hit: loaded three rows ago) and,
+        // in stage 2, its U^n (prefetched into L1 one row ago) are loaded between
+        // the two flux computations in stage 2 and after them in stage 1 (the
+        // faster placement of each, measured at 4096^2).
+        Q4 C0, un;
+        if (STAGE == 2) {
+            load(i, C0);
+            load_un(i, un);
         }
-        if (r >= 1) {
-            // x-faces between rows r-2 and r-1 under both columns
-            Q4 Fc;
-            hlle2(gamma, igm1, P0.a, P0.b, P0.c, P0.d, M1.a, M1.b, M1.c, M1.d, Fc.a, Fc.b, Fc.c, Fc.d);
-            if (r >= 2) {
-                const int i = i0 + r - 2;
-                // y-faces on row i: (a|b, b|a') with normal v, transverse u
-                Q4 sy = { yslope(W0.a), yslope(W0.b), yslope(W0.c), yslope(W0.d) };
-                Q4 M = { fma2(mhalf, sy.a, W0.a), fma2(mhalf, sy.b, W0.b), fma2(mhalf, sy.c, W0.c), fma2(mhalf, sy.d, W0.d) };
-                Q4 R;
-                R.a = make_float2(M.a.y, __shfl_down_sync(0xffffffffu, M.a.x, 1));
-                R.b = make_float2(M.b.y, __shfl_down_sync(0xffffffffu, M.b.x, 1));
-                R.c = make_float2(M.c.y, __shfl_down_sync(0xffffffffu, M.c.x, 1));
-                R.d = make_float2(M.d.y, __shfl_down_sync(0xffffffffu, M.d.x, 1));
-                Q4 G;  // G.b = mu flux (transverse), G.c = mv flux (normal)
-                hlle2(gamma, igm1,
-                      fma2(half, sy.a, W0.a), fma2(half, sy.c, W0.c), fma2(half, sy.b, W0.b), fma2(half, sy.d, W0.d),
-                      R.a, R.c, R.b, R.d,
-                      G.a, G.c, G.b, G.d);
-                // G(face a-1/2) from the left lane's G(b+1/2)
-                Q4 dG;
-                dG.a = sub2(G.a, make_float2(__shfl_up_sync(0xffffffffu, G.a.y, 1), G.a.x));
-                dG.b = sub2(G.b, make_float2(__shfl_up_sync(0xffffffffu, G.b.y, 1), G.b.x));
-                dG.c = sub2(G.c, make_float2(__shfl_up_sync(0xffffffffu, G.c.y, 1), G.c.x));
-                dG.d = sub2(G.d, make_float2(__shfl_up_sync(0xffffffffu, G.d.y, 1), G.d.x));
-                if (out_a) {
-                    const F2 fx = sp(dtdx), fy = sp(dtdy);
-                    Q4 s;
-                    s.a = sub2(C0.a, fma2(fx, sub2(Fc.a, Fp.a), mul2(fy, dG.a)));
-                    s.b = sub2(C0.b, fma2(fx, sub2(Fc.b, Fp.b), mul2(fy, dG.b)));
-                    s.c = sub2(C0.c, fma2(fx, sub2(Fc.c, Fp.c), mul2(fy, dG.c)));
-                    s.d = sub2(C0.d, fma2(fx, sub2(Fc.d, Fp.d), mul2(fy, dG.d)));
-                    const long long o = (long long)(i + 2) * g.pitch + (ca + 2);
-                    if (STAGE == 2) {
-                        const F2 n0 = un.a, n1 = un.b, n2 = un.c, n3 = un.d;
-                        s.a = mul2(half, add2(n0, s.a));
-                        s.b = mul2(half, add2(n1, s.b));
-                        s.c = mul2(half, add2(n2, s.c));
-                        s.d = mul2(half, add2(n3, s.d));
-                        if (REPAIR) {
-                            // FP64 positivity repair, element by element (rare)
-                            auto fix = [&](float& r0, float& m1, float& m2, float& e3) {
-                                const double fl = 1e-10;
-                                double r_ = (double)r0, rr = smax(r_, fl);
-                                double u_ = (double)m1 / rr, v_ = (double)m2 / rr;
-                                double keD = 0.5 * rr * (u_ * u_ + v_ * v_);
-                                double pD = (g.gamma - 1.0) * ((double)e3 - keD);
-                                if (!(r_ >= fl) || !(pD >= fl)) {
-                                    r0 = (float)rr;
-                                    e3 = (float)smax((double)e3, keD + fl / (g.gamma - 1.0));
-                                    atomicAdd(&a.ctrl->repairs, 1u);
-                                }
-                            };
-                            fix(s.a.x, s.b.x, s.c.x, s.d.x);
-                            if (out_b) fix(s.a.y, s.b.y, s.c.y, s.d.y);
+        // y-faces on row i: (a|b, b|a') with normal v, transverse u
+        Q4 sy = { yslope(Wq.a), yslope(Wq.b), yslope(Wq.c), yslope(Wq.d) };
+        Q4 Py = q_fma(half, sy, Wq), My = q_fma(mhalf, sy, Wq);
+        Q4 R;
+        R.a = make_float2(My.a.y, __shfl_down_sync(0xffffffffu, My.a.x, 1));
+        R.b = make_float2(My.b.y, __shfl_down_sync(0xffffffffu, My.b.x, 1));
+        R.c = make_float2(My.c.y, __shfl_down_sync(0xffffffffu, My.c.x, 1));
+        R.d = make_float2(My.d.y, __shfl_down_sync(0xffffffffu, My.d.x, 1));
+        Q4 G;  // G.b = mu flux (transverse), G.c = mv flux (normal)
+        hlle2(gamma, igm1, sy_, Py.a, Py.c, Py.b, Py.d, R.a, R.c, R.b, R.d, G.a, G.c, G.b, G.d);
+        // G(face a-1/2) from the left lane's G(b+1/2)
+        Q4 dG;
+        dG.a = sub2(G.a, make_float2(__shfl_up_sync(0xffffffffu, G.a.y, 1), G.a.x));
+        dG.b = sub2(G.b, make_float2(__shfl_up_sync(0xffffffffu, G.b.y, 1), G.b.x));
+        dG.c = sub2(G.c, make_float2(__shfl_up_sync(0xffffffffu, G.c.y, 1), G.c.x));
+        dG.d = sub2(G.d, make_float2(__shfl_up_sync(0xffffffffu, G.d.y, 1), G.d.x));
+
+        if (STAGE == 1) load(i, C0);
+        if (out_a) {
+            Q4 s;
+            if (STAGE == 1) {  // U1 = U - (dF + dG)
+                s.a = sub2(add2(C0.a, Fm.a), add2(Fc.a, dG.a));
+                s.b = sub2(add2(C0.b, Fm.b), add2(Fc.b, dG.b));
+                s.c = sub2(add2(C0.c, Fm.c), add2(Fc.c, dG.c));
+                s.d = sub2(add2(C0.d, Fm.d), add2(Fc.d, dG.d));
+            } else {  // U^{n+1} = (U^n + U1)/2 - (dF + dG)/2, fluxes already halved
+                s.a = fma2(half, add2(un.a, C0.a), sub2(sub2(Fm.a, Fc.a), dG.a));
+                s.b = fma2(half, add2(un.b, C0.b), sub2(sub2(Fm.b, Fc.b), dG.b));
+                s.c = fma2(half, add2(un.c, C0.c), sub2(sub2(Fm.c, Fc.c), dG.c));
+                s.d = fma2(half, add2(un.d, C0.d), sub2(sub2(Fm.d, Fc.d), dG.d));
+            }
+            const long long o = (long long)(i + 2) * pitch + (ca + 2);
+            if (STAGE == 2) {
+                // wave speeds |u|+c, |v|+c of the new state with the floors of compute_dt_2d
+                F2 rho = max2(s.a, 1e-10f);
+                F2 ir = rcp2(rho);
+                F2 u = mul2(s.b, ir), v = mul2(s.c, ir);
+                F2 ke = mul2(mul2(half, rho), fma2(v, v, mul2(u, u)));
+                F2 pr = mul2(sp(gm1), sub2(s.d, ke));
+                if (REPAIR) {
+                    // FP64 positivity repair: a cell with rho < 1e-10 or an FP64
+                    // pressure below 1e-10 gets rho >= 1e-10 and E raised to
+                    // ke + 1e-10/(gamma-1).  The FP32 pressure differs from the
+                    // FP64 one by far less than 1e-5 (gamma-1)(|E| + ke), so only
+                    // cells under that bound (near vacuum) take the FP64 path.
+                    auto fix = [&](float& r0, float& m1, float& m2, float& e3) {
+                        const double fl = 1e-10;
+                        double r_ = (double)r0, rr = smax(r_, fl);
+                        double u_ = (double)m1 / rr, v_ = (double)m2 / rr;
+                        double keD = 0.5 * rr * (u_ * u_ + v_ * v_);
+                        double pD = (g.gamma - 1.0) * ((double)e3 - keD);
+                        if (!(r_ >= fl) || !(pD >= fl)) {
+                            r0 = (float)rr;
+                            e3 = (float)smax((double)e3, keD + fl / (g.gamma - 1.0));
+                            atomicAdd(&a.ctrl->repairs, 1u);
                         }
-                        // wave speeds |u|+c, |v|+c with the floors of compute_dt_2d
-                        F2 rho = max2(s.a, 1e-10f);
-                        F2 ir = rcp2(rho);
-                        F2 u = mul2(s.b, ir), v = mul2(s.c, ir);
-                        F2 ke = mul2(mul2(half, rho), fma2(v, v, mul2(u, u)));
-                        F2 pp = max2(mul2(sp(gm1), sub2(s.d, ke)), 1e-10f);
-                        F2 gp = mul2(sp(gamma), pp);
-                        F2 c = mul2(gp, rsq2(mul2(gp, rho)));
-                        smx = fmaxf(smx, fabsf(u.x) + c.x);
-                        smy = fmaxf(smy, fabsf(v.x) + c.x);
-                        if (out_b) {
-                            smx = fmaxf(smx, fabsf(u.y) + c.y);
-                            smy = fmaxf(smy, fabsf(v.y) + c.y);
-                        }
-                        if (a.partials) {
-                            t0 += (double)s.a.x; t1 += (double)s.b.x; t2 += (double)s.c.x; t3 += (double)s.d.x;
-                            if (out_b) {
-                                t0 += (double)s.a.y; t1 += (double)s.b.y; t2 += (double)s.c.y; t3 += (double)s.d.y;
-                            }
-                        }
+                    };
+                    F2 tol = fma2(sp(1e-5f * gm1), add2(make_float2(fabsf(s.d.x), fabsf(s.d.y)), ke), sp(1e-10f));
+                    const bool near_x = !(s.a.x >= 1e-10f) || !(pr.x >= tol.x);
+                    const bool near_y = out_b && (!(s.a.y >= 1e-10f) || !(pr.y >= tol.y));
+                    if (near_x || near_y) {
+                        if (near_x) fix(s.a.x, s.b.x, s.c.x, s.d.x);
+                        if (near_y) fix(s.a.y, s.b.y, s.c.y, s.d.y);
+                        rho = max2(s.a, 1e-10f);
+                        ir = rcp2(rho);
+                        u = mul2(s.b, ir); v = mul2(s.c, ir);
+                        ke = mul2(mul2(half, rho), fma2(v, v, mul2(u, u)));
+                        pr = mul2(sp(gm1), sub2(s.d, ke));
                     }
-                    float* Uo = a.Uout;
+                }
+                F2 pp = max2(pr, 1e-10f);
+                F2 gp = mul2(sp(gamma), pp);
+                F2 c = mul2(gp, rsq2(mul2(gp, rho)));
+                F2 au = add2(make_float2(fabsf(u.x), fabsf(u.y)), c);
+                F2 av = add2(make_float2(fabsf(v.x), fabsf(v.y)), c);
+                if (!out_b) { au.y = 0.f; av.y = 0.f; }
+                smx = max3f(smx, au.x, au.y);
+                smy = max3f(smy, av.x, av.y);
+                if (TOT) {
+                    t0 += (double)s.a.x; t1 += (double)s.b.x; t2 += (double)s.c.x; t3 += (double)s.d.x;
                     if (out_b) {
-                        *reinterpret_cast<F2*>(Uo + o) = s.a;
-                        *reinterpret_cast<F2*>(Uo + vs + o) = s.b;
-                        *reinterpret_cast<F2*>(Uo + 2 * vs + o) = s.c;
-                        *reinterpret_cast<F2*>(Uo + 3 * vs + o) = s.d;
-                    } else {
-                        Uo[o] = s.a.x; Uo[vs + o] = s.b.x; Uo[2 * vs + o] = s.c.x; Uo[3 * vs + o] = s.d.x;
-                    }
-                    if (i < 2 || i >= g.nx - 2 || ca < 2 || ca + 1 >= g.ny - 2) {
-                        store_ghosts(Uo, g, 0, i, ca, s.a.x); store_ghosts(Uo, g, 1, i, ca, s.b.x);
-                        store_ghosts(Uo, g, 2, i, ca, s.c.x); store_ghosts(Uo, g, 3, i, ca, s.d.x);
-                        if (out_b) {
-                            store_ghosts(Uo, g, 0, i, ca + 1, s.a.y); store_ghosts(Uo, g, 1, i, ca + 1, s.b.y);
-                            store_ghosts(Uo, g, 2, i, ca + 1, s.c.y); store_ghosts(Uo, g, 3, i, ca + 1, s.d.y);
-                        }
+                        t0 += (double)s.a.y; t1 += (double)s.b.y; t2 += (double)s.c.y; t3 += (double)s.d.y;
                     }
                 }
             }
-            Fp = Fc;
+            float* Uo = a.Uout;
+            if (out_b) {
+                *reinterpret_cast<F2*>(Uo + o) = s.a;
+                *reinterpret_cast<F2*>(Uo + vs + o) = s.b;
+                *reinterpret_cast<F2*>(Uo + 2 * vs + o) = s.c;
+                *reinterpret_cast<F2*>(Uo + 3 * vs + o) = s.d;
+            } else {
+                Uo[o] = s.a.x; Uo[vs + o] = s.b.x; Uo[2 * vs + o] = s.c.x; Uo[3 * vs + o] = s.d.x;
+            }
+            if (GHOST && (edge_col || i < 2 || i >= nx - 2)) {
+                store_ghosts(Uo, g, 0, i, ca, s.a.x); store_ghosts(Uo, g, 1, i, ca, s.b.x);
+                store_ghosts(Uo, g, 2, i, ca, s.c.x); store_ghosts(Uo, g, 3, i, ca, s.d.x);
+                if (out_b) {
+                    store_ghosts(Uo, g, 0, i, ca + 1, s.a.y); store_ghosts(Uo, g, 1, i, ca + 1, s.b.y);
+                    store_ghosts(Uo, g, 2, i, ca + 1, s.c.y); store_ghosts(Uo, g, 3, i, ca + 1, s.d.y);
+                }
+            }
         }
-        W0 = W1; W1 = W2; P0 = P1;
+        Fm = Fc;
+        Pq = q_fma(half, S1, Wq1);
+        Wq = Wq1;
+        Wq1 = W2;
     }
     if (STAGE == 2) {
         double mx = warp_max((double)smx), my = warp_max((double)smy);
@@ -297,10 +372,10 @@ __device__ __forceinline__ void x2_body(const StageArgs<float>& a, int strip, in
             atomic_max_speed(&a.ctrl->maxs[a.p ^ 1][0], mx);
             atomic_max_speed(&a.ctrl->maxs[a.p ^ 1][1], my);
         }
-        if (a.partials) {
+        if (TOT) {
             t0 = warp_sum(t0); t1 = warp_sum(t1); t2 = warp_sum(t2); t3 = warp_sum(t3);
             if (lane == 0) {
-                long long wid = ((long long)tile_row * ((g.ny + STRIP2 - 1) / STRIP2) + strip) * 4;  // per-domain slot
+                long long wid = ((long long)tile_row * ((ny + STRIP2 - 1) / STRIP2) + strip) * 4;  // per-domain slot
                 a.partials[wid + 0] = t0; a.partials[wid + 1] = t1;
                 a.partials[wid + 2] = t2; a.partials[wid + 3] = t3;
             }
@@ -308,52 +383,99 @@ __device__ __forceinline__ void x2_body(const StageArgs<float>& a, int strip, in
     }
 }
 
-// Register budgets of the plain (no repair) stage kernels, from a sweep at
-// 4096^2 (B200, 16-row tiles, one warp per block): stage 2 under
-// __launch_bounds__(256) alone measured 0.341 ms per launch; with an explicit
-// budget of 120-128 it measured 0.243-0.247 ms, and 0.35 ms again at 118 and
-// below.  Stage 1 measured 0.218-0.220 ms for every budget from 116 to 128.
+// Register budgets of the plain (no repair) stage kernels, from sweeps at
+// 4096^2 (B200, 16-row tiles, one warp per block): 128 registers (16 warps per
+// SM) for both stages measured 0.205 / 0.223 ms per launch; budgets of 104-120
+// (17-19 warps) ran 7-18 % slower and 144 (14 warps) 15 % slower in stage 1.
 #ifndef NEST_X2_REGS1
 #define NEST_X2_REGS1 128
 #endif
 #ifndef NEST_X2_REGS2
-#define NEST_X2_REGS2 124
+#define NEST_X2_REGS2 128
 #endif
 
 __global__ void __maxnreg__(NEST_X2_REGS1) k2d_f32x2_1(StageArgs<float> a) {
-    x2_body<1, false>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+    x2_body<1, false, false, true>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
 }
+template <bool TOT>
 __global__ void __maxnreg__(NEST_X2_REGS2) k2d_f32x2_2(StageArgs<float> a) {
-    x2_body<2, false>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+    x2_body<2, false, TOT, true>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
 }
 
 // Positivity-repair variants (FP64 repair branch; rarely taken).
-template <int STAGE>
-__global__ void __launch_bounds__(256) k2d_f32x2_repair(StageArgs<float> a) {
-    x2_body<STAGE, true>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+template <int STAGE, bool TOT>
+__global__ void __maxnreg__(128) k2d_f32x2_repair(StageArgs<float> a) {
+    x2_body<STAGE, true, TOT, true>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
 }
 
-// Out-of-line copy of the per-warp body for the batched loop: keeping the
-// work-list loop's state out of the body's register allocation halves the
-// batched kernel's register count (about 128 instead of about 195).
-template <int STAGE, bool REPAIR>
-__device__ __noinline__ void x2_body_call(const StageArgs<float>& a, int strip, int tile_row) {
-    x2_body<STAGE, REPAIR>(a, strip, tile_row);
-}
+// Arguments of one batched work item: the problem's geometry stays in global
+// memory (the body copies the few fields its row loop needs).
+struct X2View {
+    const float* Uin;
+    const float* Un;
+    float* Uout;
+    const Geo2D& g;
+    const LoopParams& lp;
+    StepCtrl* ctrl;
+    double* partials;
+    int p;
+    int tx;
+};
 
 // Persistent batched stage: every warp walks the work list (problem, strip,
-// tile row) with a stride of the whole grid's warp count.
-template <int STAGE, bool REPAIR>
-__global__ void __launch_bounds__(256) kbatch_f32x2(BatchArgs<float> b) {
+// tile row) with a stride of the whole grid's warp count.  The 128-register
+// budget matches the single-domain kernels (16 warps per SM).  The ghost rings
+// are filled afterwards by kbatch_ghosts: with many small problems a large
+// share of the warps sit on a domain edge, and one copy pass over all rings
+// costs less than the edge branch inside the row loop.
+template <int STAGE, bool REPAIR, bool TOT>
+__global__ void __maxnreg__(128) kbatch_f32x2(BatchArgs<float> b) {
     const int nw = gridDim.x * blockDim.y;
     for (int it = blockIdx.x * blockDim.y + threadIdx.y; it < b.nitems; it += nw) {
         const int4 w = b.items[it];
         const BatchProblem& P = b.probs[w.x];
-        StageArgs<float> a{STAGE == 1 ? b.U + P.off : b.U1 + P.off, STAGE == 2 ? b.U + P.off : nullptr,
-                           STAGE == 1 ? b.U1 + P.off : b.U + P.off, P.g, b.lp, b.ctrls + w.x,
-                           (STAGE == 2 && b.partials) ? b.partials + 4ll * P.item0 : nullptr, b.p, b.tx};
-        x2_body_call<STAGE, REPAIR>(a, w.y, w.z);
+        const long long off = P.off;
+        X2View v{STAGE == 1 ? b.U + off : b.U1 + off, STAGE == 2 ? b.U + off : nullptr,
+                 STAGE == 1 ? b.U1 + off : b.U + off, P.g, b.lp, b.ctrls + w.x,
+                 TOT ? b.partials + 4ll * P.item0 : nullptr, b.p, b.tx};
+        x2_body<STAGE, REPAIR, TOT, false>(v, w.y, w.z);
     }
+}
+
+// Ghost rings of every problem of a batch (block row y = problem): rows -2,
+// -1, nx, nx+1 under the interior columns and columns -2, -1, ny, ny+1 beside
+// the interior rows, copied from the cells nest's periodic copy or the
+// zero-gradient copy name (the corners are never read: the stencil is a
+// cross).  Rows filled by a halo exchange are left alone.
+__global__ void __launch_bounds__(256) kbatch_ghosts(float* base, const BatchProblem* probs, int nprobs) {
+  for (int pb = blockIdx.y; pb < nprobs; pb += gridDim.y) {
+    const BatchProblem& P = probs[pb];
+    const Geo2D& g = P.g;
+    float* U = base + P.off;
+    const int nx = g.nx, ny = g.ny;
+    const long long vs = g.vstride;
+    const int nrow = 4 * ny, ntot = nrow + 4 * nx;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntot; t += gridDim.x * blockDim.x) {
+        int di, dj, si, sj;
+        if (t < nrow) {  // ghost rows, consecutive threads along a row
+            const int r = t / ny;
+            dj = sj = t - r * ny;
+            di = r < 2 ? r - 2 : nx + r - 2;
+            if ((di < 0 && g.xlo_ex) || (di >= nx && g.xhi_ex)) continue;
+            si = g.bcx == BC_PERIODIC ? (di < 0 ? di + nx : di - nx) : (di < 0 ? 0 : nx - 1);
+        } else {  // ghost columns, four consecutive threads per row
+            const int u = t - nrow, c = u & 3;
+            di = si = u >> 2;
+            dj = c < 2 ? c - 2 : ny + c - 2;
+            sj = g.bcy == BC_PERIODIC ? (dj < 0 ? dj + ny : dj - ny) : (dj < 0 ? 0 : ny - 1);
+        }
+        const long long d = g.at(di, dj), s = g.at(si, sj);
+        U[d] = U[s];
+        U[vs + d] = U[vs + s];
+        U[2 * vs + d] = U[2 * vs + s];
+        U[3 * vs + d] = U[3 * vs + s];
+    }
+  }
 }
 
 }  // namespace
@@ -363,20 +485,27 @@ int strips_f32x2(int ny) { return (ny + STRIP2 - 1) / STRIP2; }
 cudaError_t launch_batch_f32x2(const BatchArgs<float>& b, bool repair, int which, int blocks, int warps,
                                cudaStream_t st) {
     dim3 blk(32, warps);
-    BatchArgs<float> b1 = b, b2 = b;
-    if (repair) {
-        if (which & 1) kbatch_f32x2<1, true><<<blocks, blk, 0, st>>>(b1);
-        if (which & 2) kbatch_f32x2<2, true><<<blocks, blk, 0, st>>>(b2);
-    } else {
-        if (which & 1) kbatch_f32x2<1, false><<<blocks, blk, 0, st>>>(b1);
-        if (which & 2) kbatch_f32x2<2, false><<<blocks, blk, 0, st>>>(b2);
+    const bool tot = b.partials != nullptr;
+    // ghost-ring pass: enough 256-thread blocks per problem for its largest ring
+    const dim3 ggrid(b.ghost_blocks, b.nprobs < 65535 ? b.nprobs : 65535);
+    if (which & 1) {
+        if (repair) kbatch_f32x2<1, true, false><<<blocks, blk, 0, st>>>(b);
+        else kbatch_f32x2<1, false, false><<<blocks, blk, 0, st>>>(b);
+        kbatch_ghosts<<<ggrid, 256, 0, st>>>(b.U1, b.probs, b.nprobs);
+    }
+    if (which & 2) {
+        if (repair && tot) kbatch_f32x2<2, true, true><<<blocks, blk, 0, st>>>(b);
+        else if (repair) kbatch_f32x2<2, true, false><<<blocks, blk, 0, st>>>(b);
+        else if (tot) kbatch_f32x2<2, false, true><<<blocks, blk, 0, st>>>(b);
+        else kbatch_f32x2<2, false, false><<<blocks, blk, 0, st>>>(b);
+        kbatch_ghosts<<<ggrid, 256, 0, st>>>(b.U, b.probs, b.nprobs);
     }
     return cudaGetLastError();
 }
 
 int batch_max_blocks_f32x2(int warps) {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kbatch_f32x2<2, false>, 32 * warps, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kbatch_f32x2<2, true, true>, 32 * warps, 0);
     return nb;
 }
 
@@ -387,12 +516,16 @@ cudaError_t launch_2d_step_f32x2(float* U, float* U1, const Geo2D& g, const Loop
     dim3 b(32, warps), gr((nstrips + warps - 1) / warps, (g.nx + tx - 1) / tx);
     StageArgs<float> a1{U, nullptr, U1, g, lp, ctrl, nullptr, p, tx};
     StageArgs<float> a2{U1, U, Uout ? Uout : U, g, lp, ctrl, partials, p, tx};
-    if (repair) {
-        if (which & 1) k2d_f32x2_repair<1><<<gr, b, 0, st>>>(a1);
-        if (which & 2) k2d_f32x2_repair<2><<<gr, b, 0, st>>>(a2);
-    } else {
-        if (which & 1) k2d_f32x2_1<<<gr, b, 0, st>>>(a1);
-        if (which & 2) k2d_f32x2_2<<<gr, b, 0, st>>>(a2);
+    const bool tot = partials != nullptr;
+    if (which & 1) {
+        if (repair) k2d_f32x2_repair<1, false><<<gr, b, 0, st>>>(a1);
+        else k2d_f32x2_1<<<gr, b, 0, st>>>(a1);
+    }
+    if (which & 2) {
+        if (repair && tot) k2d_f32x2_repair<2, true><<<gr, b, 0, st>>>(a2);
+        else if (repair) k2d_f32x2_repair<2, false><<<gr, b, 0, st>>>(a2);
+        else if (tot) k2d_f32x2_2<true><<<gr, b, 0, st>>>(a2);
+        else k2d_f32x2_2<false><<<gr, b, 0, st>>>(a2);
     }
     return cudaGetLastError();
 }

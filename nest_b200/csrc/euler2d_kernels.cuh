@@ -331,7 +331,18 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
                         s1 = T(0.5) * (N0.b + s1);
                         s2 = T(0.5) * (N0.c + s2);
                         s3 = T(0.5) * (N0.d + s3);
-                        if (REPAIR) {
+                        // FP32 form: the FP64 repair below can only trigger for cells
+                        // whose FP32 pressure is under 1e-5 (gamma-1)(|E| + ke) (the
+                        // FP32 rounding error is far smaller), so other cells skip it.
+                        bool near = true;
+                        if (REPAIR && !Pol<T>::exact) {
+                            T r32 = smax(s0, T(1e-10)), ir32 = Pol<T>::rcp(r32);
+                            T u32 = s1 * ir32, v32 = s2 * ir32;
+                            T ke32 = ke2(r32, u32, v32);
+                            T p32 = gm1 * (s3 - ke32);
+                            near = !(s0 >= T(1e-10)) || !(p32 >= T(1e-10) + T(1e-5) * gm1 * (fabs(s3) + ke32));
+                        }
+                        if (REPAIR && near) {
                             // positivity repair of the new state in FP64
                             const double fl = 1e-10;
                             double r_ = (double)s0;
@@ -409,6 +420,8 @@ struct BatchArgs {
     LoopParams lp;
     int p;
     int tx;
+    int nprobs;                 // number of problems
+    int ghost_blocks;           // FP32 ghost-ring pass: blocks per problem
 };
 
 // Ghost ring (faces and corners) and wave-speed maxima of the current state
