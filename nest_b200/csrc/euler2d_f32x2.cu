@@ -65,6 +65,23 @@ __device__ __forceinline__ Q4 q_fma(F2 h, const Q4& s, const Q4& w) {
     return { fma2(h, s.a, w.a), fma2(h, s.b, w.b), fma2(h, s.c, w.c), fma2(h, s.d, w.d) };
 }
 
+// Per-lane asynchronous global -> shared copies (cp.async, 8 bytes: one
+// column pair of one variable).  A copy holds no registers while in flight.
+__device__ __forceinline__ void cp8(F2* smem_dst, const float* gsrc) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Shared-memory row rings of one warp: RING_U slots of the stage input and,
+// in stage 2, RING_N slots of U^n; a slot holds the lane's pair of the four
+// variables, [var][lane] so that a warp's 8-byte accesses are contiguous.
+constexpr int RING_U = 4, RING_N = 2;
+__host__ __device__ constexpr int ring_f2_per_warp(int stage) { return (RING_U + (stage == 2 ? RING_N : 0)) * 4 * 32; }
+extern __shared__ F2 x2_ring[];
+
 // cons -> prim on a pair: (rho, mu, mv, E) -> (rho, u, v, p), p >= 0.
 template <bool REPAIR>
 __device__ __forceinline__ Q4 prim2(const Q4& U, float gm1) {
@@ -77,7 +94,13 @@ __device__ __forceinline__ Q4 prim2(const Q4& U, float gm1) {
     w.d = max2(mul2(sp(gm1), sub2(U.d, ke)), 0.f);
     if (REPAIR) {
         const float fl = 1e-10f;
-        if (!(w.a.x >= fl) || !(w.d.x >= fl) || !(w.a.y >= fl) || !(w.d.y >= fl)) {
+        // one compare on the smallest of the four (min.NaN keeps a NaN); the
+        // vote over the active lanes keeps the rare FP64 path a real branch
+        float m;
+        asm("min.NaN.f32 %0, %1, %2, %3;" : "=f"(m) : "f"(w.a.x), "f"(w.a.y), "f"(w.d.x));
+        asm("min.NaN.f32 %0, %1, %2;" : "=f"(m) : "f"(m), "f"(w.d.y));
+        const bool need = !(m >= fl);
+        if (__any_sync(__activemask(), need) && need) {
             Prim4<float> p0 = cons2prim<float, true>(U.a.x, U.b.x, U.c.x, U.d.x, gm1);
             Prim4<float> p1 = cons2prim<float, true>(U.a.y, U.b.y, U.c.y, U.d.y, gm1);
             w.a = make_float2(p0.r, p1.r); w.b = make_float2(p0.u, p1.u);
@@ -132,6 +155,12 @@ __device__ __forceinline__ F2 yslope(F2 w) {
     return make_float2(mm(e.x, e.y), mm(e.y, ra - w.y));
 }
 
+// Element offset of a work item's arrays from the argument bases: zero for a
+// single domain, the problem's offset in a batch.
+__device__ __forceinline__ long long view_offset(const StageArgs<float>&) { return 0; }
+template <class A>
+__device__ __forceinline__ long long view_offset(const A& a) { return a.off; }
+
 // One warp's work: the rows of tile `tile_row` under column strip `strip`.
 // The warp owning strip 0 / tile 0 publishes the step's dt for the domain.
 //
@@ -141,7 +170,7 @@ __device__ __forceinline__ F2 yslope(F2 w) {
 // x-flux of face q+1/2 and the y-fluxes of row q, and updates row q.  Fluxes
 // come out of hlle2 already multiplied by dt/dx (dt/dy), and by 1/2 in stage
 // 2, where the Heun average is folded into the update.
-template <int STAGE, bool REPAIR, bool TOT, bool GHOST, class A>
+template <int STAGE, bool REPAIR, bool TOT, bool GHOST, bool STG, class A>
 __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
     const Geo2D& g = a.g;
     const int lane = threadIdx.x & 31;
@@ -177,9 +206,9 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
     const int j0 = strip * STRIP2;
     if (j0 >= ny) return;  // whole warp idle
     const int ca = j0 - 2 + 2 * lane;  // first of the lane's two columns
-    // element offset of the pair within a row; pairs past the ghost ring read
-    // the row padding (finite, discarded)
-    const int coff = min(ca + 2, pitch - 2);
+    // element offset of the pair within a row (plus the problem's offset in a
+    // batch); pairs past the ghost ring read the row padding (finite, discarded)
+    const long long coff = view_offset(a) + min(ca + 2, pitch - 2);
     const bool lane_out = lane >= 1 && lane <= 30;
     const bool out_a = lane_out && ca < ny;
     const bool out_b = lane_out && ca + 1 < ny;
@@ -191,6 +220,7 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
     const long long vs = g.vstride;
     const float* __restrict__ Ui = a.Uin;
     const float* Unp = a.Un;
+    float* const Uo = a.Uout;
 
     auto load = [&](int i, Q4& q) {
         const long long o = (long long)(min(i, last_row) + 2) * pitch + coff;
@@ -215,12 +245,44 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
     };
     const F2 half = sp(0.5f), mhalf = sp(-0.5f);
 
+    // STG: input rows are staged through this warp's shared-memory rings
+    // (row r of the stage input in slot r & 3, row r of U^n in slot r & 1),
+    // issued three rows (U^n: one row) ahead of their use.
+    F2* const ring = x2_ring + (STG ? threadIdx.y * ring_f2_per_warp(STAGE) + lane : 0);
+    auto stage_row = [&](int i) {
+        const float* q = Ui + (long long)(min(i, last_row) + 2) * pitch + coff;
+        F2* d = ring + (i & (RING_U - 1)) * 128;
+        cp8(d, q); cp8(d + 32, q + vs); cp8(d + 64, q + 2 * vs); cp8(d + 96, q + 3 * vs);
+    };
+    auto stage_un = [&](int i) {
+        const float* q = Unp + (long long)(min(i, last_row) + 2) * pitch + coff;
+        F2* d = ring + RING_U * 128 + (i & (RING_N - 1)) * 128;
+        cp8(d, q); cp8(d + 32, q + vs); cp8(d + 64, q + 2 * vs); cp8(d + 96, q + 3 * vs);
+    };
+    auto ring_row = [&](int i, Q4& q) {
+        const F2* d = ring + (i & (RING_U - 1)) * 128;
+        q.a = d[0]; q.b = d[32]; q.c = d[64]; q.d = d[96];
+    };
+    auto ring_un = [&](int i, Q4& q) {
+        const F2* d = ring + RING_U * 128 + (i & (RING_N - 1)) * 128;
+        q.a = d[0]; q.b = d[32]; q.c = d[64]; q.d = d[96];
+    };
+
     // prologue: rows i0-2 .. i0+1, x-flux of face i0-1/2
     Q4 Wq, Wq1, Pq, Fm, nxt;
     {
         Q4 c0, c1, c2, c3;
-        load(i0 - 2, c0); load(i0 - 1, c1); load(i0, c2); load(i0 + 1, c3);
-        load(i0 + 2, nxt);
+        load(i0 - 2, c0); load(i0 - 1, c1);
+        if (STG) {
+            stage_row(i0); stage_row(i0 + 1); stage_row(i0 + 2);
+            if (STAGE == 2) stage_un(i0);
+            cp_commit();
+            cp_wait<0>();
+            ring_row(i0, c2); ring_row(i0 + 1, c3);
+        } else {
+            load(i0, c2); load(i0 + 1, c3);
+            load(i0 + 2, nxt);
+        }
         Q4 Wa = prim2<REPAIR>(c0, gm1), Wb = prim2<REPAIR>(c1, gm1);
         Wq = prim2<REPAIR>(c2, gm1); Wq1 = prim2<REPAIR>(c3, gm1);
         Q4 Sb = minmod_pair(Wa, Wb, Wq), Sq = minmod_pair(Wb, Wq, Wq1);
@@ -229,17 +291,26 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
         Pq = q_fma(half, Sq, Wq);
     }
 
-    if (STAGE == 2) prefetch_un(i0);
+    if (STAGE == 2 && !STG) prefetch_un(i0);
     float smx = 0.f, smy = 0.f;
     double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
 #pragma unroll 1
     for (int k = 0; k < rows; ++k) {
         const int i = i0 + k;
-        Q4 cur = nxt;
-        load(i + 3, nxt);
-        // stage 2: U^n of the next row is pulled into L1 one iteration ahead
-        // and loaded after the flux work, so it holds no registers meanwhile
-        if (STAGE == 2 && k + 1 < rows) prefetch_un(i + 1);
+        Q4 cur;
+        if (STG) {
+            stage_row(i + 3);
+            if (STAGE == 2) stage_un(i + 1);
+            cp_commit();
+            cp_wait<1>();  // the group issued one row ago (row i+2, U^n row i) has landed
+            ring_row(i + 2, cur);
+        } else {
+            cur = nxt;
+            load(i + 3, nxt);
+            // stage 2: U^n of the next row is pulled into L1 one iteration ahead
+            // and loaded after the flux work, so it holds no registers meanwhile
+            if (STAGE == 2 && k + 1 < rows) prefetch_un(i + 1);
+        }
 
         // x-face i+1/2 from rows i .. i+2
         Q4 W2 = prim2<REPAIR>(cur, gm1);
@@ -254,8 +325,13 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
         // faster placement of each, measured at 4096^2).
         Q4 C0, un;
         if (STAGE == 2) {
-            load(i, C0);
-            load_un(i, un);
+            if (STG) {
+                ring_row(i, C0);
+                ring_un(i, un);
+            } else {
+                load(i, C0);
+                load_un(i, un);
+            }
         }
         // y-faces on row i: (a|b, b|a') with normal v, transverse u
         Q4 sy = { yslope(Wq.a), yslope(Wq.b), yslope(Wq.c), yslope(Wq.d) };
@@ -274,7 +350,10 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
         dG.c = sub2(G.c, make_float2(__shfl_up_sync(0xffffffffu, G.c.y, 1), G.c.x));
         dG.d = sub2(G.d, make_float2(__shfl_up_sync(0xffffffffu, G.d.y, 1), G.d.x));
 
-        if (STAGE == 1) load(i, C0);
+        if (STAGE == 1) {
+            if (STG) ring_row(i, C0);
+            else load(i, C0);
+        }
         if (out_a) {
             Q4 s;
             if (STAGE == 1) {  // U1 = U - (dF + dG)
@@ -288,7 +367,7 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
                 s.c = fma2(half, add2(un.c, C0.c), sub2(sub2(Fm.c, Fc.c), dG.c));
                 s.d = fma2(half, add2(un.d, C0.d), sub2(sub2(Fm.d, Fc.d), dG.d));
             }
-            const long long o = (long long)(i + 2) * pitch + (ca + 2);
+            const long long o = (long long)(i + 2) * pitch + coff;  // = ca + 2 on output lanes
             if (STAGE == 2) {
                 // wave speeds |u|+c, |v|+c of the new state with the floors of compute_dt_2d
                 F2 rho = max2(s.a, 1e-10f);
@@ -317,7 +396,7 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
                     F2 tol = fma2(sp(1e-5f * gm1), add2(make_float2(fabsf(s.d.x), fabsf(s.d.y)), ke), sp(1e-10f));
                     const bool near_x = !(s.a.x >= 1e-10f) || !(pr.x >= tol.x);
                     const bool near_y = out_b && (!(s.a.y >= 1e-10f) || !(pr.y >= tol.y));
-                    if (near_x || near_y) {
+                    if (__any_sync(__activemask(), near_x || near_y) && (near_x || near_y)) {
                         if (near_x) fix(s.a.x, s.b.x, s.c.x, s.d.x);
                         if (near_y) fix(s.a.y, s.b.y, s.c.y, s.d.y);
                         rho = max2(s.a, 1e-10f);
@@ -342,7 +421,6 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
                     }
                 }
             }
-            float* Uo = a.Uout;
             if (out_b) {
                 *reinterpret_cast<F2*>(Uo + o) = s.a;
                 *reinterpret_cast<F2*>(Uo + vs + o) = s.b;
@@ -352,11 +430,11 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
                 Uo[o] = s.a.x; Uo[vs + o] = s.b.x; Uo[2 * vs + o] = s.c.x; Uo[3 * vs + o] = s.d.x;
             }
             if (GHOST && (edge_col || i < 2 || i >= nx - 2)) {
-                store_ghosts(Uo, g, 0, i, ca, s.a.x); store_ghosts(Uo, g, 1, i, ca, s.b.x);
-                store_ghosts(Uo, g, 2, i, ca, s.c.x); store_ghosts(Uo, g, 3, i, ca, s.d.x);
+                store_ghosts(Uo + view_offset(a), g, 0, i, ca, s.a.x); store_ghosts(Uo + view_offset(a), g, 1, i, ca, s.b.x);
+                store_ghosts(Uo + view_offset(a), g, 2, i, ca, s.c.x); store_ghosts(Uo + view_offset(a), g, 3, i, ca, s.d.x);
                 if (out_b) {
-                    store_ghosts(Uo, g, 0, i, ca + 1, s.a.y); store_ghosts(Uo, g, 1, i, ca + 1, s.b.y);
-                    store_ghosts(Uo, g, 2, i, ca + 1, s.c.y); store_ghosts(Uo, g, 3, i, ca + 1, s.d.y);
+                    store_ghosts(Uo + view_offset(a), g, 0, i, ca + 1, s.a.y); store_ghosts(Uo + view_offset(a), g, 1, i, ca + 1, s.b.y);
+                    store_ghosts(Uo + view_offset(a), g, 2, i, ca + 1, s.c.y); store_ghosts(Uo + view_offset(a), g, 3, i, ca + 1, s.d.y);
                 }
             }
         }
@@ -387,6 +465,9 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
 // 4096^2 (B200, 16-row tiles, one warp per block): 128 registers (16 warps per
 // SM) for both stages measured 0.205 / 0.223 ms per launch; budgets of 104-120
 // (17-19 warps) ran 7-18 % slower and 144 (14 warps) 15 % slower in stage 1.
+#ifndef NEST_X2_STG
+#define NEST_X2_STG true
+#endif
 #ifndef NEST_X2_REGS1
 #define NEST_X2_REGS1 128
 #endif
@@ -395,25 +476,28 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
 #endif
 
 __global__ void __maxnreg__(NEST_X2_REGS1) k2d_f32x2_1(StageArgs<float> a) {
-    x2_body<1, false, false, true>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+    x2_body<1, false, false, true, NEST_X2_STG>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
 }
 template <bool TOT>
 __global__ void __maxnreg__(NEST_X2_REGS2) k2d_f32x2_2(StageArgs<float> a) {
-    x2_body<2, false, TOT, true>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+    x2_body<2, false, TOT, true, NEST_X2_STG>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
 }
 
 // Positivity-repair variants (FP64 repair branch; rarely taken).
 template <int STAGE, bool TOT>
 __global__ void __maxnreg__(128) k2d_f32x2_repair(StageArgs<float> a) {
-    x2_body<STAGE, true, TOT, true>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+    x2_body<STAGE, true, TOT, true, NEST_X2_STG>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
 }
 
-// Arguments of one batched work item: the problem's geometry stays in global
-// memory (the body copies the few fields its row loop needs).
+// Arguments of one batched work item: the array bases are the batch's (kernel
+// parameters), `off` is the problem's element offset, and the problem's
+// geometry stays in global memory (the body copies the few fields its row
+// loop needs).
 struct X2View {
     const float* Uin;
     const float* Un;
     float* Uout;
+    long long off;
     const Geo2D& g;
     const LoopParams& lp;
     StepCtrl* ctrl;
@@ -435,10 +519,10 @@ __global__ void __maxnreg__(128) kbatch_f32x2(BatchArgs<float> b) {
         const int4 w = b.items[it];
         const BatchProblem& P = b.probs[w.x];
         const long long off = P.off;
-        X2View v{STAGE == 1 ? b.U + off : b.U1 + off, STAGE == 2 ? b.U + off : nullptr,
-                 STAGE == 1 ? b.U1 + off : b.U + off, P.g, b.lp, b.ctrls + w.x,
+        X2View v{STAGE == 1 ? b.U : b.U1, STAGE == 2 ? b.U : nullptr, STAGE == 1 ? b.U1 : b.U, off, P.g, b.lp,
+                 b.ctrls + w.x,
                  TOT ? b.partials + 4ll * P.item0 : nullptr, b.p, b.tx};
-        x2_body<STAGE, REPAIR, TOT, false>(v, w.y, w.z);
+        x2_body<STAGE, REPAIR, TOT, false, NEST_X2_STG>(v, w.y, w.z);
     }
 }
 
@@ -478,6 +562,11 @@ __global__ void __launch_bounds__(256) kbatch_ghosts(float* base, const BatchPro
   }
 }
 
+// Dynamic shared memory of a stage launch: the row rings of its warps.
+size_t ring_bytes(int stage, int warps) {
+    return NEST_X2_STG ? (size_t)warps * ring_f2_per_warp(stage) * sizeof(F2) : 0;
+}
+
 }  // namespace
 
 int strips_f32x2(int ny) { return (ny + STRIP2 - 1) / STRIP2; }
@@ -486,18 +575,19 @@ cudaError_t launch_batch_f32x2(const BatchArgs<float>& b, bool repair, int which
                                cudaStream_t st) {
     dim3 blk(32, warps);
     const bool tot = b.partials != nullptr;
+    const size_t sm1 = ring_bytes(1, warps), sm2 = ring_bytes(2, warps);
     // ghost-ring pass: enough 256-thread blocks per problem for its largest ring
     const dim3 ggrid(b.ghost_blocks, b.nprobs < 65535 ? b.nprobs : 65535);
     if (which & 1) {
-        if (repair) kbatch_f32x2<1, true, false><<<blocks, blk, 0, st>>>(b);
-        else kbatch_f32x2<1, false, false><<<blocks, blk, 0, st>>>(b);
+        if (repair) kbatch_f32x2<1, true, false><<<blocks, blk, sm1, st>>>(b);
+        else kbatch_f32x2<1, false, false><<<blocks, blk, sm1, st>>>(b);
         kbatch_ghosts<<<ggrid, 256, 0, st>>>(b.U1, b.probs, b.nprobs);
     }
     if (which & 2) {
-        if (repair && tot) kbatch_f32x2<2, true, true><<<blocks, blk, 0, st>>>(b);
-        else if (repair) kbatch_f32x2<2, true, false><<<blocks, blk, 0, st>>>(b);
-        else if (tot) kbatch_f32x2<2, false, true><<<blocks, blk, 0, st>>>(b);
-        else kbatch_f32x2<2, false, false><<<blocks, blk, 0, st>>>(b);
+        if (repair && tot) kbatch_f32x2<2, true, true><<<blocks, blk, sm2, st>>>(b);
+        else if (repair) kbatch_f32x2<2, true, false><<<blocks, blk, sm2, st>>>(b);
+        else if (tot) kbatch_f32x2<2, false, true><<<blocks, blk, sm2, st>>>(b);
+        else kbatch_f32x2<2, false, false><<<blocks, blk, sm2, st>>>(b);
         kbatch_ghosts<<<ggrid, 256, 0, st>>>(b.U, b.probs, b.nprobs);
     }
     return cudaGetLastError();
@@ -505,7 +595,7 @@ cudaError_t launch_batch_f32x2(const BatchArgs<float>& b, bool repair, int which
 
 int batch_max_blocks_f32x2(int warps) {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kbatch_f32x2<2, true, true>, 32 * warps, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kbatch_f32x2<2, true, true>, 32 * warps, ring_bytes(2, warps));
     return nb;
 }
 
@@ -517,15 +607,16 @@ cudaError_t launch_2d_step_f32x2(float* U, float* U1, const Geo2D& g, const Loop
     StageArgs<float> a1{U, nullptr, U1, g, lp, ctrl, nullptr, p, tx};
     StageArgs<float> a2{U1, U, Uout ? Uout : U, g, lp, ctrl, partials, p, tx};
     const bool tot = partials != nullptr;
+    const size_t sm1 = ring_bytes(1, warps), sm2 = ring_bytes(2, warps);
     if (which & 1) {
-        if (repair) k2d_f32x2_repair<1, false><<<gr, b, 0, st>>>(a1);
-        else k2d_f32x2_1<<<gr, b, 0, st>>>(a1);
+        if (repair) k2d_f32x2_repair<1, false><<<gr, b, sm1, st>>>(a1);
+        else k2d_f32x2_1<<<gr, b, sm1, st>>>(a1);
     }
     if (which & 2) {
-        if (repair && tot) k2d_f32x2_repair<2, true><<<gr, b, 0, st>>>(a2);
-        else if (repair) k2d_f32x2_repair<2, false><<<gr, b, 0, st>>>(a2);
-        else if (tot) k2d_f32x2_2<true><<<gr, b, 0, st>>>(a2);
-        else k2d_f32x2_2<false><<<gr, b, 0, st>>>(a2);
+        if (repair && tot) k2d_f32x2_repair<2, true><<<gr, b, sm2, st>>>(a2);
+        else if (repair) k2d_f32x2_repair<2, false><<<gr, b, sm2, st>>>(a2);
+        else if (tot) k2d_f32x2_2<true><<<gr, b, sm2, st>>>(a2);
+        else k2d_f32x2_2<false><<<gr, b, sm2, st>>>(a2);
     }
     return cudaGetLastError();
 }
