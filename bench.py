@@ -50,7 +50,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["riemann2d"], default="riemann2d")
     ap.add_argument("--n", type=int, default=4096, help="cells per axis")
-    ap.add_argument("--forms", default="f32,f64", help="forms to time; the first is the headline")
+    ap.add_argument("--forms", default="f32,f32plain,f64",
+                    help="forms to time (f32: FP32 with FP64 totals and repair; f32plain: FP32 without them; "
+                         "f64: the plain FP64 form); the first is the headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
@@ -206,13 +208,30 @@ def alg_bytes_per_cell(form: str):
     """Algorithmic HBM bytes per cell of one launch: stage 1 reads U^n and
     writes U1 (8 values); stage 2 reads U1 and U^n and writes U^{n+1}
     (12 values).  Per cell-update that is 2.5 * 4 vars * s bytes."""
-    s = 4 if form == "f32" else 8
+    s = 4 if form.startswith("f32") else 8
     return {"stage1": 8 * s, "stage2": 12 * s, "per_cell_update": 10 * s}
+
+
+def form_args(form: str):
+    """(precision, solver flags) of a timed form: `f32` is the FP32 form with
+    FP64 conserved totals every step and FP64 positivity repair, `f32plain`
+    the same arithmetic without them, `f64` the plain FP64 form."""
+    import nest_b200 as nb
+    return {"f32": (nb.F32, nb.FLAG_TOTALS | nb.FLAG_REPAIR), "f32plain": (nb.F32, 0),
+            "f64": (nb.F64, 0)}[form]
+
+
+def tune_form(form: str) -> str:
+    return "f32" if form.startswith("f32") else "f64"
 
 
 def kernel_name(form: str, stage: str) -> str:
     """Name of the stage kernel the bench's form launches (no repair flag)."""
-    return ("k2d_f32x2_" if form == "f32" else "k2d_f64_") + stage[-1]
+    if form == "f32":  # FP64 repair; FP64 totals in stage 2
+        return "k2d_f32x2<1, true, false>" if stage == "stage1" else "k2d_f32x2<2, true, true>"
+    if form == "f32plain":
+        return f"k2d_f32x2<{stage[-1]}, false, false>"
+    return "k2d_f64_" + stage[-1]
 
 
 def traffic_from_profiles(form: str, n: int):
@@ -237,12 +256,12 @@ def run_slabs(args, ws, rank, form, cfl, st):
     from nest_b200.shard import gpu_domain
     from nest_b200.tuning import best_tiling
     n = args.n
-    prec = nb.F32 if form == "f32" else nb.F64
-    dom, ranges = gpu_domain(ws * n, n, bc=nb.BC_OUTFLOW, precision=prec, group=dist.group.WORLD)
+    prec, flags = form_args(form)
+    dom, ranges = gpu_domain(ws * n, n, bc=nb.BC_OUTFLOW, precision=prec, flags=flags, group=dist.group.WORLD)
     (slab,), ((x0, nl),) = dom.slabs, ranges
     U = riemann_2d(ws * n, n, rows=(x0, nl))
-    U = U.astype(np.float32) if form == "f32" else U
-    tiling = tuple(int(v) for v in args.tiling.split(",")) if args.tiling else best_tiling(form, nl, n)
+    U = U.astype(np.float32) if prec == nb.F32 else U
+    tiling = tuple(int(v) for v in args.tiling.split(",")) if args.tiling else best_tiling(tune_form(form), nl, n)
     slab.solver.set_tiling(*tiling)
     sst = slab.stream_obj
     slab.solver.upload(U)
@@ -283,7 +302,7 @@ def run_slabs(args, ws, rank, form, cfl, st):
     out = {"ms": ms, "k1": k1, "k2": k2, "tsim": tsim, "steps": nst, "tiling": tiling, "window": (t0, t1),
            "cells_local": nl * n, "graph_ms": None}
     if not args.no_e2e:
-        tdt = torch.float32 if form == "f32" else torch.float64
+        tdt = torch.float32 if prec == nb.F32 else torch.float64
         hin = torch.empty(U.shape, dtype=tdt, pin_memory=True)
         hin.numpy()[...] = U
         hout = torch.empty(U.shape, dtype=tdt, pin_memory=True)
@@ -354,10 +373,10 @@ def run_ours(args, ws, rank, local):
             if "e2e" in r:
                 results[form]["e2e"] = r["e2e"]
             continue
-        prec = nb.F32 if form == "f32" else nb.F64
-        U = U64.astype(np.float32) if form == "f32" else U64
-        s = nb.Solver(2, n, n, bc=nb.BC_OUTFLOW, precision=prec, stream=st.cuda_stream)
-        tiling = tuple(int(v) for v in args.tiling.split(",")) if args.tiling else best_tiling(form, n, n)
+        prec, flags = form_args(form)
+        U = U64.astype(np.float32) if prec == nb.F32 else U64
+        s = nb.Solver(2, n, n, bc=nb.BC_OUTFLOW, precision=prec, flags=flags, stream=st.cuda_stream)
+        tiling = tuple(int(v) for v in args.tiling.split(",")) if args.tiling else best_tiling(tune_form(form), n, n)
         s.set_tiling(*tiling)
         s.upload(U)
         s.step(args.warmup, cfl)
@@ -409,9 +428,10 @@ def run_ours(args, ws, rank, local):
         s.close()
         del s
     clocks.stop()
-    if "f32" in rho_final and "f64" in rho_final:
-        d = np.abs(rho_final["f32"] - rho_final["f64"])
-        results["f32"]["rho_vs_f64"] = {"max_abs": float(d.max()), "l1": float(d.mean())}
+    for f in ("f32", "f32plain"):
+        if f in rho_final and "f64" in rho_final:
+            d = np.abs(rho_final[f] - rho_final["f64"])
+            results[f]["rho_vs_f64"] = {"max_abs": float(d.max()), "l1": float(d.mean())}
     rho_final.clear()
     head = forms[0]
     r = results[head]
@@ -421,14 +441,18 @@ def run_ours(args, ws, rank, local):
     out = {
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": head, "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32" if head.startswith("f32") else "f64", "data": "synthetic",
         "config": {"workload": f"riemann2d {ws * n}x{n} {head}", "nx": ws * n, "ny": n,
+                   "form": {"f32": "FP32 state and arithmetic; FP64 conserved totals every step, FP64 time and "
+                                   "dt, FP64 positivity repair",
+                            "f32plain": "FP32 state and arithmetic; FP64 time and dt",
+                            "f64": "plain FP64 form (bit for bit with the CPU oracle)"}[head],
                    "patches": f"{n // 256}x{n // 256} of 256^2" if n % 256 == 0 else "one",
                    "bc": "outflow", "cfl": cfl, "gamma": 1.4,
                    "parallelism": "one GPU" if ws == 1 and not args.slab_path else
                    f"{ws} x-slabs of {n}x{n} (NCCL halo rows + wave-speed all-reduce)",
                    "l2": "inputs larger than L2 (two state buffers of %.0f MB each)" % (
-                       4 * (n + 4) ** 2 * (4 if head == "f32" else 8) / 1e6)},
+                       4 * (n + 4) ** 2 * (4 if head.startswith("f32") else 8) / 1e6)},
         "roofline": r["roofline"],
         "forms": results,
         "e2e": r.get("e2e"),

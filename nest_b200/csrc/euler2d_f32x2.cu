@@ -78,9 +78,37 @@ __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0
 // Shared-memory row rings of one warp: RING_U slots of the stage input and,
 // in stage 2, RING_N slots of U^n; a slot holds the lane's pair of the four
 // variables, [var][lane] so that a warp's 8-byte accesses are contiguous.
+// LOOK: rows of the stage input in flight ahead of the row march (the row
+// issued at iteration i is consumed at iteration i + LOOK - 2); U^n runs
+// LOOK - 2 rows ahead.  Measured at 4096^2: LOOK 3 0.386 ms per step, 4 and
+// 5 (8-slot rings) 0.437 / 0.443 ms (the larger rings cost warps per SM).
+constexpr int LOOK = 3;
 constexpr int RING_U = 4, RING_N = 2;
+static_assert(RING_U >= LOOK + 1 && RING_N >= LOOK - 1, "ring too small for the lookahead");
 __host__ __device__ constexpr int ring_f2_per_warp(int stage) { return (RING_U + (stage == 2 ? RING_N : 0)) * 4 * 32; }
 extern __shared__ F2 x2_ring[];
+
+// 1/x for a positive double x that is an FP32 value of at least 1e-10:
+// Newton-Raphson iteration y <- y + y (1 - x y), which doubles the number of
+// correct bits per step, from the ~22-bit FP32 approximate reciprocal; two
+// steps reach double precision (to within an ulp or two).  Unlike a
+// division it needs no out-of-line slow path, so the rare FP64 branches
+// below leave the row loop free of calls.
+__device__ __forceinline__ double rcp_nr(double x) {
+    double y = (double)__fdividef(1.0f, (float)x);
+    y = fma(y, fma(-x, y, 1.0), y);
+    return fma(y, fma(-x, y, 1.0), y);
+}
+
+// FP64 primitives of one cell with the 1e-10 floors on rho and p (the FP32
+// form's near-vacuum path).
+__device__ __forceinline__ Prim4<float> prim_floor64(float U0, float U1, float U2, float U3, float gm1) {
+    const double fl = 1e-10;
+    double r = smax((double)U0, fl), ir = rcp_nr(r);
+    double u = (double)U1 * ir, v = (double)U2 * ir;
+    double pd = (double)gm1 * ((double)U3 - (0.5 * r * u * u + 0.5 * r * v * v));
+    return { (float)r, (float)u, (float)v, (float)smax(pd, fl) };
+}
 
 // cons -> prim on a pair: (rho, mu, mv, E) -> (rho, u, v, p), p >= 0.
 template <bool REPAIR>
@@ -101,8 +129,8 @@ __device__ __forceinline__ Q4 prim2(const Q4& U, float gm1) {
         asm("min.NaN.f32 %0, %1, %2;" : "=f"(m) : "f"(m), "f"(w.d.y));
         const bool need = !(m >= fl);
         if (__any_sync(__activemask(), need) && need) {
-            Prim4<float> p0 = cons2prim<float, true>(U.a.x, U.b.x, U.c.x, U.d.x, gm1);
-            Prim4<float> p1 = cons2prim<float, true>(U.a.y, U.b.y, U.c.y, U.d.y, gm1);
+            Prim4<float> p0 = prim_floor64(U.a.x, U.b.x, U.c.x, U.d.x, gm1);
+            Prim4<float> p1 = prim_floor64(U.a.y, U.b.y, U.c.y, U.d.y, gm1);
             w.a = make_float2(p0.r, p1.r); w.b = make_float2(p0.u, p1.u);
             w.c = make_float2(p0.v, p1.v); w.d = make_float2(p0.p, p1.p);
         }
@@ -170,7 +198,7 @@ __device__ __forceinline__ long long view_offset(const A& a) { return a.off; }
 // x-flux of face q+1/2 and the y-fluxes of row q, and updates row q.  Fluxes
 // come out of hlle2 already multiplied by dt/dx (dt/dy), and by 1/2 in stage
 // 2, where the Heun average is folded into the update.
-template <int STAGE, bool REPAIR, bool TOT, bool GHOST, bool STG, class A>
+template <int STAGE, bool REPAIR, bool TOT, bool GHOST, class A>
 __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
     const Geo2D& g = a.g;
     const int lane = threadIdx.x & 31;
@@ -195,6 +223,7 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
         if (!a.ctrl->active[a.p]) return;
         dt = a.ctrl->dt[a.p];
     }
+    const double gmd = g.gamma - 1.0, igmd = 1.0 / gmd;  // FP64 repair constants
     const double hs = STAGE == 2 ? 0.5 : 1.0;
     const float dtdx = (float)(hs * dt / g.dx);
     const float dtdy = (float)(hs * dt / g.dy);
@@ -229,26 +258,15 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
         q.c = __ldg(reinterpret_cast<const F2*>(Ui + 2 * vs + o));
         q.d = __ldg(reinterpret_cast<const F2*>(Ui + 3 * vs + o));
     };
-    auto load_un = [&](int i, Q4& q) {
-        const long long o = (long long)(i + 2) * pitch + coff;
-        q.a = *reinterpret_cast<const F2*>(Unp + o);
-        q.b = *reinterpret_cast<const F2*>(Unp + vs + o);
-        q.c = *reinterpret_cast<const F2*>(Unp + 2 * vs + o);
-        q.d = *reinterpret_cast<const F2*>(Unp + 3 * vs + o);
-    };
-    auto prefetch_un = [&](int i) {
-        const float* q = Unp + (long long)(i + 2) * pitch + coff;
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(q + vs));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(q + 2 * vs));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(q + 3 * vs));
-    };
     const F2 half = sp(0.5f), mhalf = sp(-0.5f);
 
-    // STG: input rows are staged through this warp's shared-memory rings
-    // (row r of the stage input in slot r & 3, row r of U^n in slot r & 1),
-    // issued three rows (U^n: one row) ahead of their use.
-    F2* const ring = x2_ring + (STG ? threadIdx.y * ring_f2_per_warp(STAGE) + lane : 0);
+    // Input rows are staged through this warp's shared-memory rings (row r of
+    // the stage input in slot r & 3, row r of U^n in slot r & 1), issued
+    // three rows (U^n: one row) ahead of their use.  Before staging (loads
+    // into registers one row ahead, the update's re-read of its own row from
+    // L1) ncu measured a 10 % L1 hit rate on that re-read and long-scoreboard
+    // waits as the top stall, at 0.434 ms per 4096^2 step against 0.386.
+    F2* const ring = x2_ring + threadIdx.y * ring_f2_per_warp(STAGE) + lane;
     auto stage_row = [&](int i) {
         const float* q = Ui + (long long)(min(i, last_row) + 2) * pitch + coff;
         F2* d = ring + (i & (RING_U - 1)) * 128;
@@ -269,20 +287,16 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
     };
 
     // prologue: rows i0-2 .. i0+1, x-flux of face i0-1/2
-    Q4 Wq, Wq1, Pq, Fm, nxt;
+    Q4 Wq, Wq1, Pq, Fm;
     {
         Q4 c0, c1, c2, c3;
         load(i0 - 2, c0); load(i0 - 1, c1);
-        if (STG) {
-            stage_row(i0); stage_row(i0 + 1); stage_row(i0 + 2);
-            if (STAGE == 2) stage_un(i0);
-            cp_commit();
-            cp_wait<0>();
-            ring_row(i0, c2); ring_row(i0 + 1, c3);
-        } else {
-            load(i0, c2); load(i0 + 1, c3);
-            load(i0 + 2, nxt);
-        }
+        for (int r = 0; r < LOOK; ++r) stage_row(i0 + r);
+        if (STAGE == 2)
+            for (int r = 0; r < LOOK - 2; ++r) stage_un(i0 + r);
+        cp_commit();
+        cp_wait<0>();
+        ring_row(i0, c2); ring_row(i0 + 1, c3);
         Q4 Wa = prim2<REPAIR>(c0, gm1), Wb = prim2<REPAIR>(c1, gm1);
         Wq = prim2<REPAIR>(c2, gm1); Wq1 = prim2<REPAIR>(c3, gm1);
         Q4 Sb = minmod_pair(Wa, Wb, Wq), Sq = minmod_pair(Wb, Wq, Wq1);
@@ -291,26 +305,17 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
         Pq = q_fma(half, Sq, Wq);
     }
 
-    if (STAGE == 2 && !STG) prefetch_un(i0);
     float smx = 0.f, smy = 0.f;
     double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
 #pragma unroll 1
     for (int k = 0; k < rows; ++k) {
         const int i = i0 + k;
         Q4 cur;
-        if (STG) {
-            stage_row(i + 3);
-            if (STAGE == 2) stage_un(i + 1);
-            cp_commit();
-            cp_wait<1>();  // the group issued one row ago (row i+2, U^n row i) has landed
-            ring_row(i + 2, cur);
-        } else {
-            cur = nxt;
-            load(i + 3, nxt);
-            // stage 2: U^n of the next row is pulled into L1 one iteration ahead
-            // and loaded after the flux work, so it holds no registers meanwhile
-            if (STAGE == 2 && k + 1 < rows) prefetch_un(i + 1);
-        }
+        stage_row(i + LOOK);
+        if (STAGE == 2) stage_un(i + LOOK - 2);
+        cp_commit();
+        cp_wait<LOOK - 2>();  // row i+2 (and U^n row i) have landed
+        ring_row(i + 2, cur);
 
         // x-face i+1/2 from rows i .. i+2
         Q4 W2 = prim2<REPAIR>(cur, gm1);
@@ -319,19 +324,13 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
         Q4 Fc;
         hlle2(gamma, igm1, sx, Pq.a, Pq.b, Pq.c, Pq.d, M1.a, M1.b, M1.c, M1.d, Fc.a, Fc.b, Fc.c, Fc.d);
 
-        // The conserved values of row i (an L1 hit: loaded three rows ago) and,
-        // in stage 2, its U^n (prefetched into L1 one row ago) are loaded between
-        // the two flux computations in stage 2 and after them in stage 1 (the
-        // faster placement of each, measured at 4096^2).
+        // The conserved values of row i and, in stage 2, its U^n are read from
+        // the rings between the two flux computations in stage 2 and after
+        // them in stage 1 (the faster placement of each, measured at 4096^2).
         Q4 C0, un;
         if (STAGE == 2) {
-            if (STG) {
-                ring_row(i, C0);
-                ring_un(i, un);
-            } else {
-                load(i, C0);
-                load_un(i, un);
-            }
+            ring_row(i, C0);
+            ring_un(i, un);
         }
         // y-faces on row i: (a|b, b|a') with normal v, transverse u
         Q4 sy = { yslope(Wq.a), yslope(Wq.b), yslope(Wq.c), yslope(Wq.d) };
@@ -350,10 +349,7 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
         dG.c = sub2(G.c, make_float2(__shfl_up_sync(0xffffffffu, G.c.y, 1), G.c.x));
         dG.d = sub2(G.d, make_float2(__shfl_up_sync(0xffffffffu, G.d.y, 1), G.d.x));
 
-        if (STAGE == 1) {
-            if (STG) ring_row(i, C0);
-            else load(i, C0);
-        }
+        if (STAGE == 1) ring_row(i, C0);
         if (out_a) {
             Q4 s;
             if (STAGE == 1) {  // U1 = U - (dF + dG)
@@ -383,13 +379,13 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
                     // cells under that bound (near vacuum) take the FP64 path.
                     auto fix = [&](float& r0, float& m1, float& m2, float& e3) {
                         const double fl = 1e-10;
-                        double r_ = (double)r0, rr = smax(r_, fl);
-                        double u_ = (double)m1 / rr, v_ = (double)m2 / rr;
+                        double r_ = (double)r0, rr = smax(r_, fl), irr = rcp_nr(rr);
+                        double u_ = (double)m1 * irr, v_ = (double)m2 * irr;
                         double keD = 0.5 * rr * (u_ * u_ + v_ * v_);
-                        double pD = (g.gamma - 1.0) * ((double)e3 - keD);
+                        double pD = gmd * ((double)e3 - keD);
                         if (!(r_ >= fl) || !(pD >= fl)) {
                             r0 = (float)rr;
-                            e3 = (float)smax((double)e3, keD + fl / (g.gamma - 1.0));
+                            e3 = (float)smax((double)e3, keD + fl * igmd);
                             atomicAdd(&a.ctrl->repairs, 1u);
                         }
                     };
@@ -461,32 +457,14 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
     }
 }
 
-// Register budgets of the plain (no repair) stage kernels, from sweeps at
-// 4096^2 (B200, 16-row tiles, one warp per block): 128 registers (16 warps per
-// SM) for both stages measured 0.205 / 0.223 ms per launch; budgets of 104-120
-// (17-19 warps) ran 7-18 % slower and 144 (14 warps) 15 % slower in stage 1.
-#ifndef NEST_X2_STG
-#define NEST_X2_STG true
-#endif
-#ifndef NEST_X2_REGS1
-#define NEST_X2_REGS1 128
-#endif
-#ifndef NEST_X2_REGS2
-#define NEST_X2_REGS2 128
-#endif
-
-__global__ void __maxnreg__(NEST_X2_REGS1) k2d_f32x2_1(StageArgs<float> a) {
-    x2_body<1, false, false, true, NEST_X2_STG>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
-}
-template <bool TOT>
-__global__ void __maxnreg__(NEST_X2_REGS2) k2d_f32x2_2(StageArgs<float> a) {
-    x2_body<2, false, TOT, true, NEST_X2_STG>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
-}
-
-// Positivity-repair variants (FP64 repair branch; rarely taken).
-template <int STAGE, bool TOT>
-__global__ void __maxnreg__(128) k2d_f32x2_repair(StageArgs<float> a) {
-    x2_body<STAGE, true, TOT, true, NEST_X2_STG>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+// Single-domain stage kernels: STAGE 1 or 2, REPAIR = FP64 positivity repair,
+// TOT = per-warp FP64 totals (stage 2).  All run under a 128-register budget
+// (16 warps per SM): from sweeps at 4096^2 (B200, 16-row tiles, one warp per
+// block), budgets of 104-120 (17-19 warps) ran 7-18 % slower and 144 (14
+// warps) 15 % slower in stage 1.
+template <int STAGE, bool REPAIR, bool TOT>
+__global__ void __maxnreg__(128) k2d_f32x2(StageArgs<float> a) {
+    x2_body<STAGE, REPAIR, TOT, true>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
 }
 
 // Arguments of one batched work item: the array bases are the batch's (kernel
@@ -522,7 +500,7 @@ __global__ void __maxnreg__(128) kbatch_f32x2(BatchArgs<float> b) {
         X2View v{STAGE == 1 ? b.U : b.U1, STAGE == 2 ? b.U : nullptr, STAGE == 1 ? b.U1 : b.U, off, P.g, b.lp,
                  b.ctrls + w.x,
                  TOT ? b.partials + 4ll * P.item0 : nullptr, b.p, b.tx};
-        x2_body<STAGE, REPAIR, TOT, false, NEST_X2_STG>(v, w.y, w.z);
+        x2_body<STAGE, REPAIR, TOT, false>(v, w.y, w.z);
     }
 }
 
@@ -564,7 +542,7 @@ __global__ void __launch_bounds__(256) kbatch_ghosts(float* base, const BatchPro
 
 // Dynamic shared memory of a stage launch: the row rings of its warps.
 size_t ring_bytes(int stage, int warps) {
-    return NEST_X2_STG ? (size_t)warps * ring_f2_per_warp(stage) * sizeof(F2) : 0;
+    return (size_t)warps * ring_f2_per_warp(stage) * sizeof(F2);
 }
 
 }  // namespace
@@ -609,14 +587,14 @@ cudaError_t launch_2d_step_f32x2(float* U, float* U1, const Geo2D& g, const Loop
     const bool tot = partials != nullptr;
     const size_t sm1 = ring_bytes(1, warps), sm2 = ring_bytes(2, warps);
     if (which & 1) {
-        if (repair) k2d_f32x2_repair<1, false><<<gr, b, sm1, st>>>(a1);
-        else k2d_f32x2_1<<<gr, b, sm1, st>>>(a1);
+        if (repair) k2d_f32x2<1, true, false><<<gr, b, sm1, st>>>(a1);
+        else k2d_f32x2<1, false, false><<<gr, b, sm1, st>>>(a1);
     }
     if (which & 2) {
-        if (repair && tot) k2d_f32x2_repair<2, true><<<gr, b, sm2, st>>>(a2);
-        else if (repair) k2d_f32x2_repair<2, false><<<gr, b, sm2, st>>>(a2);
-        else if (tot) k2d_f32x2_2<true><<<gr, b, sm2, st>>>(a2);
-        else k2d_f32x2_2<false><<<gr, b, sm2, st>>>(a2);
+        if (repair && tot) k2d_f32x2<2, true, true><<<gr, b, sm2, st>>>(a2);
+        else if (repair) k2d_f32x2<2, true, false><<<gr, b, sm2, st>>>(a2);
+        else if (tot) k2d_f32x2<2, false, true><<<gr, b, sm2, st>>>(a2);
+        else k2d_f32x2<2, false, false><<<gr, b, sm2, st>>>(a2);
     }
     return cudaGetLastError();
 }
