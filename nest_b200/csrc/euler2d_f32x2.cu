@@ -24,6 +24,7 @@ namespace {
 constexpr int STRIP2 = 60;  // output columns per warp
 
 
+
 using F2 = float2;
 
 __device__ __forceinline__ F2 sp(float a) { return make_float2(a, a); }
@@ -307,6 +308,9 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
 
     float smx = 0.f, smy = 0.f;
     double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    // Not unrolled: at 4096^2 an unroll of 2 (which removes the window
+    // rotation's register copies) gained 3 % in the plain kernels but lost
+    // 2 % in the repair + totals ones; 3 and 4 lost 12-25 %.
 #pragma unroll 1
     for (int k = 0; k < rows; ++k) {
         const int i = i0 + k;
