@@ -108,8 +108,18 @@ struct AdjSmem {
     T Sy[4][ATX][RY2];               // y slopes of columns j0-2 .. in the tile rows
     T XL[4][ATX + 3][ATY], XR[4][ATX + 3][ATY];  // x-face state adjoints, faces between rows i0-2+f, i0-1+f
     T YL[4][ATX][ATY + 3], YR[4][ATX][ATY + 3];  // y-face state adjoints, faces between columns j0-2+f, j0-1+f
+    T Uc[4][ATX][ATY];               // conserved values of the tile's own cells (kept from the load pass)
+    T Ex[4][ATX][ATY];               // Extra of the tile's cells, fetched asynchronously at the start
     signed char Bx[4][RX2][ATY], By[4][ATX][RY2];  // minmod branch: 0 none, 1 first, 2 second difference
 };
+
+// Per-thread asynchronous global -> shared copy of one value (cp.async).
+template <typename T>
+__device__ __forceinline__ void adj_cp(T* smem_dst, const T* gsrc) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    if (sizeof(T) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gsrc) : "memory");
+}
 
 // Lin = alpha * adj(U, Lout) + beta * Extra.  All arrays use the solver's
 // 2D device layout (Geo2D); periodic wrap on both axes.  Needs
@@ -147,11 +157,25 @@ __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lo
         int r = j % g.ny;
         return r < 0 ? r + g.ny : r;
     };
+    // Extra of this thread's output cell: requested now, read in the last pass
+    // (the thread reads back only what it copied itself)
+    const bool has_cell = tid < ATX * ATY && i0 + tid / ATY < g.nx && j0 + tid % ATY < g.ny;
+    if (Extra && has_cell) {
+        const int a = tid / ATY, b = tid % ATY;
+        const long long o = g.at(i0 + a, j0 + b);
+        for (int k = 0; k < 4; ++k) adj_cp(&S.Ex[k][a][b], Extra + k * vs + o);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
     for (int t = tid; t < RX3 * RY3; t += ANT) {
         int a = t / RY3, b = t % RY3;
         long long o = g.at(wrapi(i0 - 3 + a), wrapj(j0 - 3 + b));
-        Prim4<T> w = cons2prim<T, false>(U[o], U[vs + o], U[2 * vs + o], U[3 * vs + o], gm1);
+        const T u0 = U[o], u1 = U[vs + o], u2 = U[2 * vs + o], u3 = U[3 * vs + o];
+        Prim4<T> w = cons2prim<T, false>(u0, u1, u2, u3, gm1);
         W[0][a][b] = w.r; W[1][a][b] = w.u; W[2][a][b] = w.v; W[3][a][b] = w.p;
+        if (a >= 3 && a < ATX + 3 && b >= 3 && b < ATY + 3) {
+            S.Uc[0][a - 3][b - 3] = u0; S.Uc[1][a - 3][b - 3] = u1;
+            S.Uc[2][a - 3][b - 3] = u2; S.Uc[3][a - 3][b - 3] = u3;
+        }
     }
     for (int t = tid; t < RX2 * RY2; t += ANT) {
         int a = t / RY2, b = t % RY2;
@@ -232,7 +256,7 @@ __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lo
         wb[k] = v;
     }
     const long long o = g.at(i, j);
-    T rho = U[o], mu = U[vs + o], mv = U[2 * vs + o], E = U[3 * vs + o];
+    T rho = S.Uc[0][a][b], mu = S.Uc[1][a][b], mv = S.Uc[2][a][b], E = S.Uc[3][a][b];
     const T ir = T(1) / rho;
     T u = mu / rho, v = mv / rho;
     T praw = gm1 * (E - (T(0.5) * rho * u * u + T(0.5) * rho * v * v));
@@ -243,9 +267,10 @@ __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lo
     T mvb = wb[2] * ir - act * wb[3] * gm1 * v;
     T Eb = act * wb[3] * gm1;
     T out[4] = { Lo[0][a + 2][b + 2] + rb, Lo[1][a + 2][b + 2] + mub, Lo[2][a + 2][b + 2] + mvb, Lo[3][a + 2][b + 2] + Eb };
+    if (Extra) asm volatile("cp.async.wait_group 0;" ::: "memory");
     for (int k = 0; k < 4; ++k) {
         T val = out[k];
-        if (Extra) val += beta * Extra[k * vs + o];
+        if (Extra) val += beta * S.Ex[k][a][b];
         Lin[k * vs + o] = val;
     }
 }
