@@ -551,10 +551,31 @@ def bench_adjoint(args):
     fwd, bwd = st["forward_ms"], st["backward_ms"]
     fd = fd_check_1d(lambda: nb.Solver(1, n, bc=nb.BC_PERIODIC, flags=nb.FLAG_NO_RESIDENT), U0, tgt, n, K,
                      a.dts(), lam0, ndir=args.fd_directions) if args.fd_directions > 0 else None
+    # the FP32 form: FP32 forward and reverse stages on the FP64 run's loss;
+    # its gradient against the FP64 adjoint gradient
+    s32 = nb.Solver(1, n, bc=nb.BC_PERIODIC, precision=nb.F32)
+    s32.upload(U0.astype(np.float32))
+    a32 = Adjoint(s32, K, 0, 64)
+    a32.forward(0.4)  # warm
+    s32.upload(U0.astype(np.float32))
+    a32 = Adjoint(s32, K, 0, 64)
+    a32.forward(0.4)
+    UT32 = s32.download().astype(np.float64)
+    lam32 = np.zeros_like(UT32)
+    lam32[0, 2:-2] = (UT32[0, 2:-2] - tgt) / n
+    g32 = a32.backward(lam32.astype(np.float32)).astype(np.float64)[:, 2:-2]
+    st32 = a32.stats()
+    g64 = lam0[:, 2:-2]
+    f32 = {"forward_ms": st32["forward_ms"], "backward_ms": st32["backward_ms"],
+           "adjoint_over_forward": st32["backward_ms"] / st32["forward_ms"],
+           "grad_rel_l2_vs_f64": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+           "grad_cosine_vs_f64": float(np.sum(g32 * g64) / (np.linalg.norm(g32) * np.linalg.norm(g64)))}
+    a32.close()
+    s32.close()
     return {"n": n, "steps": K, "checkpoint_every": 64, "forward_ms": fwd, "backward_ms": bwd, "fd_check": fd,
             "adjoint_over_forward": bwd / fwd, "gradient_over_forward": (fwd + bwd) / fwd,
             "recomputed_steps": st["recomputed_steps"], "checkpoint_mb": st["checkpoint_bytes"] / 1e6,
-            "launches": 2 * K + 2 * K + 3 * K, "dtype": "f64"}
+            "launches": 2 * (2 * K + 2 * K + 3 * K), "dtype": "f64", "f32": f32}
 
 
 def bench_sod1d(reps: int = 20):

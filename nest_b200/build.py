@@ -3,7 +3,8 @@
 Each translation unit gets its own floating-point flags:
   euler1d.cu, euler2d_f64.cu  -fmad=false  (FP64 plain form: bit-exact with
                                             nest's CPU operation order)
-  euler2d_f32.cu              -use_fast_math (FP32 form)
+  euler1d_f32.cu, euler2d_f32*.cu
+                              -use_fast_math (FP32 form)
   capi.cpp                    host runtime and C ABI (compiled as CUDA C++)
 The library is built in-tree (nest_b200/lib/) so that it travels with the
 repository snapshot; nothing is installed into site-packages.
@@ -26,6 +27,7 @@ COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++20", "-Xcompiler", "-fPIC", "-I", 
 
 UNITS = {
     "euler1d.cu": ["-fmad=false"],
+    "euler1d_f32.cu": ["-use_fast_math"],
     "euler2d_f64.cu": ["-fmad=false"],
     "euler2d_f32.cu": ["-use_fast_math"],
     "euler2d_f32x2.cu": ["-use_fast_math"],
@@ -33,6 +35,7 @@ UNITS = {
     "capi.cpp": ["-x", "cu"],
     "noalloc.cu": [],
     "adjoint1d.cu": [],
+    "adjoint1d_f32.cu": ["-use_fast_math"],
     "adjoint.cpp": ["-x", "cu"],
     "exchange.cu": [],
     "adjoint2d.cu": [],

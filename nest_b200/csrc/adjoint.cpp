@@ -32,6 +32,9 @@ namespace nestb {
 cudaError_t launch_1d_adjoint_stage(const double* U, const double* Lout, const double* Extra, double* Lin, int n,
                                     int h, const double* dtp, double dx, double gamma, double alpha, double beta,
                                     cudaStream_t st);
+cudaError_t launch_1d_adjoint_stage_f32(const float* U, const float* Lout, const float* Extra, float* Lin, int n,
+                                        int h, const double* dtp, double dx, double gamma, double alpha, double beta,
+                                        cudaStream_t st);
 }
 
 namespace {
@@ -59,15 +62,26 @@ struct Stepper1D : Stepper {
     StepCtrl* ctrl;
     explicit Stepper1D(nest_solver* s_, StepCtrl* c) : s(s_), ctrl(c) {}
     cudaError_t stage(int which, void* Un, void* U1, void* Uout, const LoopParams& lp, int p) override {
+        if (s->d.precision == NEST_F32)
+            return launch_1d_step_f32((float*)Un, (float*)U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp, ctrl,
+                                      p, which, s->st, (float*)Uout);
         return launch_1d_step((double*)Un, (double*)U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp, ctrl, p,
                               which, s->st, (double*)Uout);
     }
     cudaError_t adjoint_step(void* Un, void* U1, const double* dtp, void* lam, void* lam_new, void* tmp) override {
-        cudaError_t e = launch_1d_adjoint_stage((const double*)U1, (const double*)lam, nullptr, (double*)tmp,
-                                                s->d.nx, s->h, dtp, s->d.dx, s->d.gamma, 0.5, 0.0, s->st);
+        const int n = s->d.nx, h = s->h;
+        if (s->d.precision == NEST_F32) {
+            cudaError_t e = launch_1d_adjoint_stage_f32((const float*)U1, (const float*)lam, nullptr, (float*)tmp, n,
+                                                        h, dtp, s->d.dx, s->d.gamma, 0.5, 0.0, s->st);
+            if (e != cudaSuccess) return e;
+            return launch_1d_adjoint_stage_f32((const float*)Un, (const float*)tmp, (const float*)lam,
+                                               (float*)lam_new, n, h, dtp, s->d.dx, s->d.gamma, 1.0, 0.5, s->st);
+        }
+        cudaError_t e = launch_1d_adjoint_stage((const double*)U1, (const double*)lam, nullptr, (double*)tmp, n, h,
+                                                dtp, s->d.dx, s->d.gamma, 0.5, 0.0, s->st);
         if (e != cudaSuccess) return e;
         return launch_1d_adjoint_stage((const double*)Un, (const double*)tmp, (const double*)lam,
-                                       (double*)lam_new, s->d.nx, s->h, dtp, s->d.dx, s->d.gamma, 1.0, 0.5, s->st);
+                                       (double*)lam_new, n, h, dtp, s->d.dx, s->d.gamma, 1.0, 0.5, s->st);
     }
 };
 
@@ -267,7 +281,6 @@ nest_status nest_adjoint_create(nest_solver* s, int nsteps, int policy, int para
     if (nsteps <= 0) return fail(NEST_ERR_INVALID, "nsteps must be positive");
     if (policy != NEST_CKPT_UNIFORM && policy != NEST_CKPT_BINOMIAL) return fail(NEST_ERR_INVALID, "bad policy");
     if (param < 1) return fail(NEST_ERR_INVALID, "checkpoint parameter must be >= 1");
-    if (s->d.dim == 1 && s->d.precision != NEST_F64) return fail(NEST_ERR_UNSUPPORTED, "adjoint: 1D runs in FP64");
     if (s->d.bc_x != NEST_BC_PERIODIC || (s->d.dim == 2 && s->d.bc_y != NEST_BC_PERIODIC))
         return fail(NEST_ERR_UNSUPPORTED, "adjoint: periodic boundaries");
     if (s->d.flags & (NEST_FLAG_SPLIT_COMPAT | NEST_FLAG_FP32_SCALAR))

@@ -71,7 +71,9 @@ LoopParams base_params(const nest_solver* s) {
 nest_status nestb::rt::prepare(nest_solver* s) {
     CK(cudaMemsetAsync(&s->ctrl->maxs[s->parity][0], 0, 2 * sizeof(unsigned long long), s->st));
     cudaError_t e;
-    if (s->d.dim == 1) {
+    if (s->d.dim == 1 && s->d.precision == NEST_F32) {
+        e = launch_1d_prepare_f32((float*)s->U, s->d.nx, s->h, s->d.gamma, s->d.bc_x, s->ctrl, s->parity, s->st);
+    } else if (s->d.dim == 1) {
         e = launch_1d_prepare((double*)s->U, s->d.nx, s->h, s->d.gamma, s->d.bc_x, s->ctrl, s->parity, s->st);
     } else if (s->d.precision == NEST_F64) {
         e = launch_2d_prepare_f64((double*)s->U, s->geo(), s->ctrl, s->parity, s->st);
@@ -85,6 +87,9 @@ nest_status nestb::rt::prepare(nest_solver* s) {
 
 // Enqueue one step (two kernels) with parity p; `which` selects the stages.
 cudaError_t nestb::rt::enqueue_step(nest_solver* s, const LoopParams& lp, int p, int which) {
+    if (s->d.dim == 1 && s->d.precision == NEST_F32)
+        return launch_1d_step_f32((float*)s->U, (float*)s->U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp,
+                                  s->ctrl, p, which, s->st);
     if (s->d.dim == 1)
         return launch_1d_step((double*)s->U, (double*)s->U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp,
                               s->ctrl, p, which, s->st);
@@ -227,7 +232,8 @@ nest_status nest_solver_create(const nest_solver_desc* d, nest_solver** out) {
     if (d->dim == 2 && d->bc_y != NEST_BC_PERIODIC && d->bc_y != NEST_BC_OUTFLOW) return fail(NEST_ERR_INVALID, "bad bc_y");
     if (d->dim == 1 && d->halo < 2) return fail(NEST_ERR_INVALID, "PLM needs a halo of at least 2");
     if (d->dim == 2 && d->halo != 2) return fail(NEST_ERR_UNSUPPORTED, "2D solver uses a halo of exactly 2");
-    if (d->dim == 1 && d->precision != NEST_F64) return fail(NEST_ERR_UNSUPPORTED, "1D solver is FP64");
+    if (d->dim == 1 && d->precision == NEST_F32 && (d->flags & (NEST_FLAG_TOTALS | NEST_FLAG_REPAIR)))
+        return fail(NEST_ERR_UNSUPPORTED, "1D FP32 solver: totals and repair are 2D options");
     if (d->precision != NEST_F64 && d->precision != NEST_F32) return fail(NEST_ERR_INVALID, "bad precision");
     if (d->dim == 2 && (long long)d->nx * d->ny > (1ll << 31)) return fail(NEST_ERR_INVALID, "domain too large");
     if ((d->flags & NEST_FLAG_SPLIT_COMPAT) && (d->dim != 2 || d->precision != NEST_F64))

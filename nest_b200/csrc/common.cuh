@@ -132,12 +132,14 @@ __device__ __forceinline__ void publish_step(StepCtrl* c, int p, const LoopParam
 // 1D numerics (3 variables), examples/sod1d/euler1d.hpp
 // ---------------------------------------------------------------------------
 
-// eos_t::pressure, euler1d.hpp:31-44.
-__device__ __forceinline__ double eos_pressure(double gm1, double rho, double mom, double erg) {
-    double u = mom / rho;
-    double ke = 0.5 * rho * u * u;
-    double p = gm1 * (erg - ke);
-    return smax(p, 0.0);
+// eos_t::pressure, euler1d.hpp:31-44.  T = double is the plain form (IEEE
+// division, nest's operation order); T = float the FP32 form.
+template <typename T>
+__device__ __forceinline__ T eos_pressure(T gm1, T rho, T mom, T erg) {
+    T u = mom / rho;
+    T ke = T(0.5) * rho * u * u;
+    T p = gm1 * (erg - ke);
+    return smax(p, T(0));
 }
 
 // minmod, euler1d.hpp:112-115.
@@ -160,24 +162,22 @@ __device__ __forceinline__ T limit(T a, T b, int lim) {
 }
 
 // hlle_flux, euler1d.hpp:178-242 (Davis speeds, three branches).
-__device__ __forceinline__ void hlle1d(double gamma, double gm1,
-                                       double rL, double uL, double pL,
-                                       double rR, double uR, double pR,
-                                       double& f0, double& f1, double& f2) {
-    double cL = sqrt(gamma * pL / rL);
-    double EL = pL / gm1 + 0.5 * rL * uL * uL;
-    double cR = sqrt(gamma * pR / rR);
-    double ER = pR / gm1 + 0.5 * rR * uR * uR;
-    double SL = smin(uL - cL, uR - cR);
-    double SR = smax(uL + cL, uR + cR);
-    double FL0 = rL * uL, FL1 = rL * uL * uL + pL, FL2 = (EL + pL) * uL;
-    double FR0 = rR * uR, FR1 = rR * uR * uR + pR, FR2 = (ER + pR) * uR;
-    if (SL >= 0.0) {
+template <typename T>
+__device__ __forceinline__ void hlle1d(T gamma, T gm1, T rL, T uL, T pL, T rR, T uR, T pR, T& f0, T& f1, T& f2) {
+    T cL = sqrt(gamma * pL / rL);
+    T EL = pL / gm1 + T(0.5) * rL * uL * uL;
+    T cR = sqrt(gamma * pR / rR);
+    T ER = pR / gm1 + T(0.5) * rR * uR * uR;
+    T SL = smin(uL - cL, uR - cR);
+    T SR = smax(uL + cL, uR + cR);
+    T FL0 = rL * uL, FL1 = rL * uL * uL + pL, FL2 = (EL + pL) * uL;
+    T FR0 = rR * uR, FR1 = rR * uR * uR + pR, FR2 = (ER + pR) * uR;
+    if (SL >= T(0)) {
         f0 = FL0; f1 = FL1; f2 = FL2;
-    } else if (SR <= 0.0) {
+    } else if (SR <= T(0)) {
         f0 = FR0; f1 = FR1; f2 = FR2;
     } else {
-        double SLR = SL * SR, dS = SR - SL;
+        T SLR = SL * SR, dS = SR - SL;
         f0 = (SR * FL0 - SL * FR0 + SLR * (rR - rL)) / dS;
         f1 = (SR * FL1 - SL * FR1 + SLR * (rR * uR - rL * uL)) / dS;
         f2 = (SR * FL2 - SL * FR2 + SLR * (ER - EL)) / dS;

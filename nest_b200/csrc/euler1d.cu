@@ -30,99 +30,136 @@ __device__ __forceinline__ int ghost_src_1d(int e, int n, int h, int bc) {
     return bc == BC_PERIODIC ? e - n : h + n - 1;
 }
 
-__device__ double block_max_1d(double v, double* red) {
-    v = warp_max(v);
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) red[w] = v;
-    __syncthreads();
-    if (w == 0) {
-        int nw = (blockDim.x + 31) >> 5;
-        double x = (l < nw) ? red[l] : 0.0;
-        x = warp_max(x);
-        if (l == 0) red[32] = x;
+// Ghost copies fed by interior cell c (0-based) of a 3-variable SoA array
+// over the extended range: nest's periodic copy or the zero-gradient copy.
+__device__ __forceinline__ void ghost_copies_1d(double* A, int nt, int n, int h, int bc, int c, double v0, double v1,
+                                                double v2) {
+    auto put = [&](int e) { A[e] = v0; A[nt + e] = v1; A[2 * nt + e] = v2; };
+    if (bc == BC_PERIODIC) {
+        if (c >= n - h) put(c + h - n);
+        if (c < h) put(h + n + c);
+    } else {
+        if (c == 0) for (int e = 0; e < h; ++e) put(e);
+        if (c == n - 1) for (int e = h + n; e < nt; ++e) put(e);
     }
-    __syncthreads();
-    double r = red[32];
-    __syncthreads();
-    return r;
 }
 
-// One stage inside the resident kernel.  Uin/Uout are shared-memory SoA
-// arrays of 3*nt; W scratch 3*nt; F scratch 3*(n+1).  If avg != nullptr the
-// result is 0.5*(avg + stage) (second Heun stage, written into avg).
-__device__ void resident_stage(const double* Uin, double* Uout, double* avg, double* W, double* F,
-                               int n, int h, double dtdx, double gamma, double gm1, int lim) {
-    int nt = n + 2 * h;
-    for (int f = threadIdx.x; f <= n; f += blockDim.x) {
-        // face between extended cells a = h+f-1 and b = h+f
-        int a = h + f - 1, b = h + f;
-        double sa[3], sb[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const double* w = W + k * nt;
-            sa[k] = limit(w[a] - w[a - 1], w[b] - w[a], lim);
-            sb[k] = limit(w[b] - w[a], w[b + 1] - w[b], lim);
-        }
-        double rL = W[a] + 0.5 * sa[0], uL = W[nt + a] + 0.5 * sa[1], pL = W[2 * nt + a] + 0.5 * sa[2];
-        double rR = W[b] - 0.5 * sb[0], uR = W[nt + b] - 0.5 * sb[1], pR = W[2 * nt + b] - 0.5 * sb[2];
-        double f0, f1, f2;
-        hlle1d(gamma, gm1, rL, uL, pL, rR, uR, pR, f0, f1, f2);
-        F[f] = f0; F[(n + 1) + f] = f1; F[2 * (n + 1) + f] = f2;
-    }
-    __syncthreads();
-    for (int c = threadIdx.x; c < n; c += blockDim.x) {
-        int e = h + c;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            double v = Uin[k * nt + e] - dtdx * (F[k * (n + 1) + c + 1] - F[k * (n + 1) + c]);
-            if (avg) avg[k * nt + e] = 0.5 * (avg[k * nt + e] + v);
-            else Uout[k * nt + e] = v;
-        }
-    }
-    __syncthreads();
-}
-
-// Primitive pass over the extended array (cons_to_prim, euler1d.hpp:69-84),
-// returning this thread's max |u|+c over interior cells (benchmark_euler1d.cpp:168-180).
-__device__ double resident_prims(const double* U, double* W, int n, int h, double gamma, double gm1) {
-    int nt = n + 2 * h;
-    double ms = 0.0;
-    for (int e = threadIdx.x; e < nt; e += blockDim.x) {
-        double rho = U[e], mom = U[nt + e], erg = U[2 * nt + e];
-        double u = mom / rho;
-        double p = eos_pressure(gm1, rho, mom, erg);
-        W[e] = rho; W[nt + e] = u; W[2 * nt + e] = p;
-        if (e >= h && e < h + n) {
-            double c = sqrt(gamma * p / rho);
-            ms = smax(ms, fabs(u) + c);
-        }
-    }
-    return ms;
-}
-
-__device__ void resident_ghosts(double* U, int n, int h, int bc) {
-    int nt = n + 2 * h;
-    for (int t = threadIdx.x; t < 3 * 2 * h; t += blockDim.x) {
-        int k = t / (2 * h), g = t % (2 * h);
-        int e = (g < h) ? g : h + n + (g - h);
-        U[k * nt + e] = U[k * nt + ghost_src_1d(e, n, h, bc)];
-    }
-    __syncthreads();
-}
-
-__global__ void __launch_bounds__(1024)
-k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int bc,
-             LoopParams lp, StepCtrl* ctrl, int p) {
+// Resident single-CTA solver: the whole extended domain lives in shared
+// memory (U, U1, primitives W, face fluxes F) and the CTA runs the complete
+// time loop.  A step is four phases separated by four barriers:
+//   faces of stage 1 (PLM + HLLE from W)        | update U1, its primitives and ghost copies |
+//   faces of stage 2 (from the primitives of U1) | Heun update of U, its primitives, ghost copies and max |u|+c
+// Each thread handles K faces / cells per phase (K >= 2: independent
+// chains of FP64 division / square root interleave).  The arithmetic of
+// every face and cell is that of nest's OpenMP loop
+// (examples/benchmark/benchmark_euler1d.cpp:113-209); primitives of a ghost
+// cell are the primitives of its source cell, which is what nest computes
+// from the copied conserved values.
+template <int K, int MAXT>
+__global__ void __launch_bounds__(MAXT)
+k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int bc, LoopParams lp, StepCtrl* ctrl,
+             int p) {
     extern __shared__ double sm[];
-    int nt = n + 2 * h;
+    const int nt = n + 2 * h, T = blockDim.x, tid = threadIdx.x;
     double* U = sm;
     double* U1 = U + 3 * nt;
     double* W = U1 + 3 * nt;
     double* F = W + 3 * nt;
     double* red = F + 3 * (n + 1);
-    double gm1 = gamma - 1.0;
-    for (int i = threadIdx.x; i < 3 * nt; i += blockDim.x) { U[i] = Ug[i]; U1[i] = 0.0; }
+    const double gm1 = gamma - 1.0;
+    const int nw = (T + 31) >> 5;
+
+    // primitives of cell value (r, m, e): u, p (cons_to_prim, euler1d.hpp:69-84)
+    auto prims_of = [&](int c, double r, double m, double e, double* Wd) {
+        const double u = m / r;
+        const double pr = eos_pressure(gm1, r, m, e);
+        const int x = h + c;
+        Wd[x] = r; Wd[nt + x] = u; Wd[2 * nt + x] = pr;
+        ghost_copies_1d(Wd, nt, n, h, bc, c, r, u, pr);
+    };
+    // max |u| + c over this thread's cells of A (benchmark_euler1d.cpp:168-180), warp maxima to red
+    auto speeds = [&]() {
+        double ms = 0.0;
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const int c = tid + q * T;
+            if (c < n) {
+                const int x = h + c;
+                const double u = W[nt + x], pr = W[2 * nt + x], r = W[x];
+                const double cs = sqrt(gamma * pr / r);
+                ms = smax(ms, fabs(u) + cs);
+            }
+        }
+        ms = warp_max(ms);
+        if ((tid & 31) == 0) red[tid >> 5] = ms;
+    };
+    auto reduce_red = [&]() {
+        double ms = 0.0;
+        for (int w = 0; w < nw; ++w) ms = smax(ms, red[w]);
+        return ms;
+    };
+    // face fluxes of the stage whose primitives are in W
+    auto faces = [&]() {
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const int f = tid + q * T;
+            if (f <= n) {
+                // face between extended cells a = h+f-1 and b = h+f
+                const int a = h + f - 1, b = h + f;
+                double sa[3], sb[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const double* w = W + k * nt;
+                    sa[k] = limit(w[a] - w[a - 1], w[b] - w[a], lp.lim);
+                    sb[k] = limit(w[b] - w[a], w[b + 1] - w[b], lp.lim);
+                }
+                const double rL = W[a] + 0.5 * sa[0], uL = W[nt + a] + 0.5 * sa[1], pL = W[2 * nt + a] + 0.5 * sa[2];
+                const double rR = W[b] - 0.5 * sb[0], uR = W[nt + b] - 0.5 * sb[1], pR = W[2 * nt + b] - 0.5 * sb[2];
+                double f0, f1, f2;
+                hlle1d(gamma, gm1, rL, uL, pL, rR, uR, pR, f0, f1, f2);
+                F[f] = f0; F[(n + 1) + f] = f1; F[2 * (n + 1) + f] = f2;
+            }
+        }
+    };
+    // stage update of this thread's cells: out = in - dtdx (F_{c+1} - F_c),
+    // or U = 0.5 (U + that) in stage 2; then the new state's primitives and ghosts
+    auto update = [&](const double* Uin, double* Uout, bool heun, double dtdx) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            const int c = tid + q * T;
+            if (c < n) {
+                const int x = h + c;
+                double v[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    v[k] = Uin[k * nt + x] - dtdx * (F[k * (n + 1) + c + 1] - F[k * (n + 1) + c]);
+                    if (heun) v[k] = 0.5 * (Uout[k * nt + x] + v[k]);
+                    Uout[k * nt + x] = v[k];
+                }
+                ghost_copies_1d(Uout, nt, n, h, bc, c, v[0], v[1], v[2]);
+                prims_of(c, v[0], v[1], v[2], W);
+            }
+        }
+    };
+
+    // prologue: state, ghosts, primitives and the first max wave speed
+    for (int i = tid; i < 3 * nt; i += T) { U[i] = Ug[i]; U1[i] = 0.0; }
     __syncthreads();
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        const int c = tid + q * T;
+        if (c < n) {
+            const int x = h + c;
+            const double r = U[x], m = U[nt + x], e = U[2 * nt + x];
+            ghost_copies_1d(U, nt, n, h, bc, c, r, m, e);
+            prims_of(c, r, m, e, W);
+        }
+    }
+    __syncthreads();
+    speeds();
+    __syncthreads();
+    double ms = reduce_red();
+
     double time = ctrl->time[p];
     int step = ctrl->step[p];
     for (int it = 0;; ++it) {
@@ -130,9 +167,6 @@ k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int
         if (lp.t_final > 0.0 && !(time < lp.t_final)) break;
         if (lp.max_steps > 0 && step >= lp.max_steps) break;
         if (lp.dts_in && step >= lp.dts_cap) break;
-        // Stage 1: ghost fill of U, primitives (+ CFL max over the interior).
-        resident_ghosts(U, n, h, bc);
-        double ms = block_max_1d(resident_prims(U, W, n, h, gamma, gm1), red);
         double dt;
         if (lp.fixed_dt > 0.0) {
             dt = lp.fixed_dt;
@@ -142,21 +176,24 @@ k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int
             dt = lp.cfl * dx / ms;
             if (lp.t_final > 0.0) dt = smin(dt, lp.t_final - time);
         }
-        if (!(ms == ms) || ms > 1.79e308) { if (threadIdx.x == 0) atomicOr(&ctrl->err, ERRW_NONFINITE); break; }
-        if (threadIdx.x == 0 && lp.dts_out && step < lp.dts_cap) lp.dts_out[step] = dt;
-        double dtdx = dt / dx;
-        resident_stage(U, U1, nullptr, W, F, n, h, dtdx, gamma, gm1, lp.lim);
-        // Stage 2 on U1, averaged into U.
-        resident_ghosts(U1, n, h, bc);
-        resident_prims(U1, W, n, h, gamma, gm1);
+        if (!(ms == ms) || ms > 1.79e308) { if (tid == 0) atomicOr(&ctrl->err, ERRW_NONFINITE); break; }
+        if (tid == 0 && lp.dts_out && step < lp.dts_cap) lp.dts_out[step] = dt;
+        const double dtdx = dt / dx;
+        faces();                        // stage 1 fluxes from W = prims(U)
         __syncthreads();
-        resident_stage(U1, nullptr, U, W, F, n, h, dtdx, gamma, gm1, lp.lim);
+        update(U, U1, false, dtdx);     // U1, W = prims(U1), ghosts
+        __syncthreads();
+        faces();                        // stage 2 fluxes
+        __syncthreads();
+        update(U1, U, true, dtdx);      // U = (U + U1 - dt L(U1)) / 2, W = prims(U), ghosts
+        speeds();
+        __syncthreads();
+        ms = reduce_red();
         time += dt;
         ++step;
     }
-    resident_ghosts(U, n, h, bc);
-    for (int i = threadIdx.x; i < 3 * nt; i += blockDim.x) Ug[i] = U[i];
-    if (threadIdx.x == 0) {
+    for (int i = tid; i < 3 * nt; i += T) Ug[i] = U[i];
+    if (tid == 0) {
         ctrl->time[p] = time; ctrl->step[p] = step;
         ctrl->time[p ^ 1] = time; ctrl->step[p ^ 1] = step;
     }
@@ -170,165 +207,41 @@ size_t resident_smem_bytes(int n, int h) {
 cudaError_t launch_1d_resident(double* U, int n, int h, double dx, double gamma, int bc,
                                const LoopParams& lp, StepCtrl* ctrl, int p, cudaStream_t st) {
     size_t smem = resident_smem_bytes(n, h);
-    cudaError_t e = cudaFuncSetAttribute(k1d_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // K faces per thread: at least two (independent FP64 chains per thread),
+    // more when n + 1 faces exceed 2 * 1024
+    const int K = (n + 1 <= 2048) ? 2 : 3;
+    if (n + 1 > 3 * 1024) return cudaErrorInvalidValue;
+    int threads = ((n + 1 + K - 1) / K + 31) / 32 * 32;
+    cudaError_t e;
+    // the thread bound sets the register budget: 640 threads (n < 1280, up to
+    // 102 registers) or 1024 (64 registers)
+    auto go = [&](auto kern) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) kern<<<1, threads, smem, st>>>(U, n, h, dx, gamma, bc, lp, ctrl, p);
+    };
+    if (K == 2 && threads <= 640) go(k1d_resident<2, 640>);
+    else if (K == 2) go(k1d_resident<2, 1024>);
+    else go(k1d_resident<3, 1024>);
     if (e != cudaSuccess) return e;
-    int nt = n + 2 * h;
-    int threads = nt >= 1024 ? 1024 : ((nt + 31) / 32) * 32;
-    k1d_resident<<<1, threads, smem, st>>>(U, n, h, dx, gamma, bc, lp, ctrl, p);
     return cudaGetLastError();
 }
 
-// ---------------------------------------------------------------------------
-// Tiled multi-CTA stage kernels
-// ---------------------------------------------------------------------------
+}  // namespace nestb
 
-constexpr int T1 = 256;  // cells per tile = threads per block
+// Tiled multi-CTA stage kernels (FP64 instantiation; euler1d_f32.cu holds the
+// FP32 one).
+#include "euler1d_tiled.cuh"
 
-// Max |u|+c of one cell (benchmark_euler1d.cpp:170-178).
-__device__ __forceinline__ double cell_speed_1d(double rho, double mom, double erg, double gamma, double gm1) {
-    double u = mom / rho;
-    double p = eos_pressure(gm1, rho, mom, erg);
-    double c = sqrt(gamma * p / rho);
-    return fabs(u) + c;
-}
-
-// Writes the ghost copies that the value of interior cell c (0-based) feeds.
-__device__ __forceinline__ void push_ghosts_1d(double* U, int nt, int k, int c, int n, int h, int bc, double v) {
-    if (bc == BC_PERIODIC) {
-        if (c < h) U[k * nt + h + n + c] = v;
-        if (c >= n - h) U[k * nt + (c - (n - h))] = v;
-    } else {
-        if (c == 0) for (int g = 0; g < h; ++g) U[k * nt + g] = v;
-        if (c == n - 1) for (int g = 0; g < h; ++g) U[k * nt + h + n + g] = v;
-    }
-}
-
-template <int STAGE>
-__global__ void __launch_bounds__(T1)
-k1d_stage(const double* __restrict__ Uin, const double* Un, double* Uout,
-          int n, int h, double dx, double gamma, int bc, LoopParams lp, StepCtrl* ctrl, int p) {
-    __shared__ double W[3][T1 + 4];
-    __shared__ double F[3][T1 + 1];
-    __shared__ double red[33];
-    int nt = n + 2 * h;
-    double gm1 = gamma - 1.0;
-    double dt;
-    if (STAGE == 1) {
-        bool done = step_is_done(ctrl, p, lp);
-        double ms = bits_speed(ctrl->maxs[p][0]);
-        double pd = done ? -1.0 : prescribed_dt(ctrl, p, lp);
-        if (pd > 0.0) dt = pd;
-        else {
-            dt = lp.cfl * dx / ms;
-            if (lp.t_final > 0.0) dt = smin(dt, lp.t_final - ctrl->time[p]);
-        }
-        if (blockIdx.x == 0 && threadIdx.x == 0) publish_step(ctrl, p, lp, done, dt);
-        if (done) return;
-    } else {
-        if (!ctrl->active[p]) return;
-        dt = ctrl->dt[p];
-    }
-    double dtdx = dt / dx;
-    int c0 = blockIdx.x * T1;  // first interior cell of the tile
-    // primitives of extended cells c0-2 .. c0+T1+1 (clamped at the array end)
-    for (int t = threadIdx.x; t < T1 + 4; t += T1) {
-        int e = min(h + c0 - 2 + t, nt - 1);
-        double rho = Uin[e], mom = Uin[nt + e], erg = Uin[2 * nt + e];
-        W[0][t] = rho;
-        W[1][t] = mom / rho;
-        W[2][t] = eos_pressure(gm1, rho, mom, erg);
-    }
-    __syncthreads();
-    int nf = min(T1, n - c0) + 1;  // faces of this tile
-    for (int f = threadIdx.x; f < nf; f += T1) {
-        int a = f + 1, b = f + 2;  // tile-local W indices around the face
-        double sa[3], sb[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            sa[k] = limit(W[k][a] - W[k][a - 1], W[k][b] - W[k][a], lp.lim);
-            sb[k] = limit(W[k][b] - W[k][a], W[k][b + 1] - W[k][b], lp.lim);
-        }
-        double f0, f1, f2;
-        hlle1d(gamma, gm1, W[0][a] + 0.5 * sa[0], W[1][a] + 0.5 * sa[1], W[2][a] + 0.5 * sa[2],
-               W[0][b] - 0.5 * sb[0], W[1][b] - 0.5 * sb[1], W[2][b] - 0.5 * sb[2], f0, f1, f2);
-        F[0][f] = f0; F[1][f] = f1; F[2][f] = f2;
-    }
-    __syncthreads();
-    int c = c0 + threadIdx.x;
-    double ms = 0.0;
-    if (c < n) {
-        int e = h + c;
-        double v[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            double s = Uin[k * nt + e] - dtdx * (F[k][threadIdx.x + 1] - F[k][threadIdx.x]);
-            v[k] = (STAGE == 1) ? s : 0.5 * (Un[k * nt + e] + s);
-        }
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            Uout[k * nt + e] = v[k];
-            push_ghosts_1d(Uout, nt, k, c, n, h, bc, v[k]);
-        }
-        if (STAGE == 2) ms = cell_speed_1d(v[0], v[1], v[2], gamma, gm1);
-    }
-    if (STAGE == 2) {
-        ms = warp_max(ms);
-        int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        if (l == 0) red[w] = ms;
-        __syncthreads();
-        if (w == 0) {
-            double x = (l < T1 / 32) ? red[l] : 0.0;
-            x = warp_max(x);
-            if (l == 0) {
-                if (!(x == x) || x > 1.79e308) atomicOr(&ctrl->err, ERRW_NONFINITE);
-                atomic_max_speed(&ctrl->maxs[p ^ 1][0], x);
-            }
-        }
-    }
-}
-
-// Ghost fill + max |u|+c of the current state into slot p (used once after
-// an upload, and by the standalone compute_dt entry point).
-__global__ void __launch_bounds__(T1)
-k1d_prepare(double* U, int n, int h, double gamma, int bc, StepCtrl* ctrl, int p, int reset) {
-    __shared__ double red[33];
-    int nt = n + 2 * h;
-    double gm1 = gamma - 1.0;
-    int c = blockIdx.x * T1 + threadIdx.x;
-    double ms = 0.0;
-    if (c < n) {
-        int e = h + c;
-        double v0 = U[e], v1 = U[nt + e], v2 = U[2 * nt + e];
-        push_ghosts_1d(U, nt, 0, c, n, h, bc, v0);
-        push_ghosts_1d(U, nt, 1, c, n, h, bc, v1);
-        push_ghosts_1d(U, nt, 2, c, n, h, bc, v2);
-        ms = cell_speed_1d(v0, v1, v2, gamma, gm1);
-    }
-    ms = warp_max(ms);
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) red[w] = ms;
-    __syncthreads();
-    if (w == 0) {
-        double x = (l < T1 / 32) ? red[l] : 0.0;
-        x = warp_max(x);
-        if (l == 0) atomic_max_speed(&ctrl->maxs[p][0], x);
-    }
-    (void)reset;
-}
+namespace nestb {
 
 cudaError_t launch_1d_prepare(double* U, int n, int h, double gamma, int bc, StepCtrl* ctrl, int p,
                               cudaStream_t st) {
-    int blocks = (n + T1 - 1) / T1;
-    k1d_prepare<<<blocks, T1, 0, st>>>(U, n, h, gamma, bc, ctrl, p, 0);
-    return cudaGetLastError();
+    return launch_1d_prepare_t<double>(U, n, h, gamma, bc, ctrl, p, st);
 }
 
 cudaError_t launch_1d_step(double* U, double* U1, int n, int h, double dx, double gamma, int bc,
                            const LoopParams& lp, StepCtrl* ctrl, int p, int which, cudaStream_t st, double* Uout) {
-    int blocks = (n + T1 - 1) / T1;
-    if (which & 1) k1d_stage<1><<<blocks, T1, 0, st>>>(U, nullptr, U1, n, h, dx, gamma, bc, lp, ctrl, p);
-    if (which & 2) k1d_stage<2><<<blocks, T1, 0, st>>>(U1, U, Uout ? Uout : U, n, h, dx, gamma, bc, lp, ctrl, p);
-    return cudaGetLastError();
+    return launch_1d_step_t<double>(U, U1, n, h, dx, gamma, bc, lp, ctrl, p, which, st, Uout);
 }
 
 }  // namespace nestb

@@ -1,0 +1,176 @@
+// Tiled multi-CTA 1D stage kernels, templated on the arithmetic type:
+// instantiated for double in euler1d.cu (-fmad=false, nest's operation order,
+// bit for bit with the OpenMP path) and for float in euler1d_f32.cu (the FP32
+// form, fast reciprocal / square root).  Time, dt and the wave-speed maximum
+// stay FP64 in both.
+//
+// One CTA of T1 threads owns T1 cells: primitives of its cells and a 2-cell
+// halo into shared memory, one HLLE per face, the update with the ghost
+// copies it feeds; stage 2 fuses the Heun average and the block's max
+// |u|+c (one atomic per block).  dt is derived on the device from that
+// maximum by the next stage 1, so a step is two launches and no host
+// synchronisation.
+#pragma once
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace nestb {
+namespace {
+
+constexpr int T1 = 256;  // cells per tile = threads per block
+
+// Max |u|+c of one cell (benchmark_euler1d.cpp:170-178).
+template <typename T>
+__device__ __forceinline__ T cell_speed_1d(T rho, T mom, T erg, T gamma, T gm1) {
+    T u = mom / rho;
+    T p = eos_pressure(gm1, rho, mom, erg);
+    T c = sqrt(gamma * p / rho);
+    return fabs(u) + c;
+}
+
+// Writes the ghost copies that the value of interior cell c (0-based) feeds.
+template <typename T>
+__device__ __forceinline__ void push_ghosts_1d(T* U, int nt, int k, int c, int n, int h, int bc, T v) {
+    if (bc == BC_PERIODIC) {
+        if (c < h) U[k * nt + h + n + c] = v;
+        if (c >= n - h) U[k * nt + (c - (n - h))] = v;
+    } else {
+        if (c == 0) for (int g = 0; g < h; ++g) U[k * nt + g] = v;
+        if (c == n - 1) for (int g = 0; g < h; ++g) U[k * nt + h + n + g] = v;
+    }
+}
+
+template <typename T, int STAGE>
+__global__ void __launch_bounds__(T1)
+k1d_stage(const T* __restrict__ Uin, const T* Un, T* Uout,
+          int n, int h, double dx, double gamma_d, int bc, LoopParams lp, StepCtrl* ctrl, int p) {
+    __shared__ T W[3][T1 + 4];
+    __shared__ T F[3][T1 + 1];
+    __shared__ double red[33];
+    int nt = n + 2 * h;
+    const T gamma = (T)gamma_d;
+    const T gm1 = (T)(gamma_d - 1.0);
+    double dt;
+    if (STAGE == 1) {
+        bool done = step_is_done(ctrl, p, lp);
+        double ms = bits_speed(ctrl->maxs[p][0]);
+        double pd = done ? -1.0 : prescribed_dt(ctrl, p, lp);
+        if (pd > 0.0) dt = pd;
+        else {
+            dt = lp.cfl * dx / ms;
+            if (lp.t_final > 0.0) dt = smin(dt, lp.t_final - ctrl->time[p]);
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) publish_step(ctrl, p, lp, done, dt);
+        if (done) return;
+    } else {
+        if (!ctrl->active[p]) return;
+        dt = ctrl->dt[p];
+    }
+    const T dtdx = (T)(dt / dx);
+    int c0 = blockIdx.x * T1;  // first interior cell of the tile
+    // primitives of extended cells c0-2 .. c0+T1+1 (clamped at the array end)
+    for (int t = threadIdx.x; t < T1 + 4; t += T1) {
+        int e = min(h + c0 - 2 + t, nt - 1);
+        T rho = Uin[e], mom = Uin[nt + e], erg = Uin[2 * nt + e];
+        W[0][t] = rho;
+        W[1][t] = mom / rho;
+        W[2][t] = eos_pressure(gm1, rho, mom, erg);
+    }
+    __syncthreads();
+    int nf = min(T1, n - c0) + 1;  // faces of this tile
+    for (int f = threadIdx.x; f < nf; f += T1) {
+        int a = f + 1, b = f + 2;  // tile-local W indices around the face
+        T sa[3], sb[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            sa[k] = limit(W[k][a] - W[k][a - 1], W[k][b] - W[k][a], lp.lim);
+            sb[k] = limit(W[k][b] - W[k][a], W[k][b + 1] - W[k][b], lp.lim);
+        }
+        T f0, f1, f2;
+        hlle1d(gamma, gm1, W[0][a] + T(0.5) * sa[0], W[1][a] + T(0.5) * sa[1], W[2][a] + T(0.5) * sa[2],
+               W[0][b] - T(0.5) * sb[0], W[1][b] - T(0.5) * sb[1], W[2][b] - T(0.5) * sb[2], f0, f1, f2);
+        F[0][f] = f0; F[1][f] = f1; F[2][f] = f2;
+    }
+    __syncthreads();
+    int c = c0 + threadIdx.x;
+    double ms = 0.0;
+    if (c < n) {
+        int e = h + c;
+        T v[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            T s = Uin[k * nt + e] - dtdx * (F[k][threadIdx.x + 1] - F[k][threadIdx.x]);
+            v[k] = (STAGE == 1) ? s : T(0.5) * (Un[k * nt + e] + s);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            Uout[k * nt + e] = v[k];
+            push_ghosts_1d(Uout, nt, k, c, n, h, bc, v[k]);
+        }
+        if (STAGE == 2) ms = (double)cell_speed_1d(v[0], v[1], v[2], gamma, gm1);
+    }
+    if (STAGE == 2) {
+        ms = warp_max(ms);
+        int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        if (l == 0) red[w] = ms;
+        __syncthreads();
+        if (w == 0) {
+            double x = (l < T1 / 32) ? red[l] : 0.0;
+            x = warp_max(x);
+            if (l == 0) {
+                if (!(x == x) || x > 1.79e308) atomicOr(&ctrl->err, ERRW_NONFINITE);
+                atomic_max_speed(&ctrl->maxs[p ^ 1][0], x);
+            }
+        }
+    }
+}
+
+// Ghost fill + max |u|+c of the current state into slot p (used once after
+// an upload, and by the standalone compute_dt entry point).
+template <typename T>
+__global__ void __launch_bounds__(T1)
+k1d_prepare(T* U, int n, int h, double gamma_d, int bc, StepCtrl* ctrl, int p) {
+    __shared__ double red[33];
+    int nt = n + 2 * h;
+    const T gamma = (T)gamma_d;
+    const T gm1 = (T)(gamma_d - 1.0);
+    int c = blockIdx.x * T1 + threadIdx.x;
+    double ms = 0.0;
+    if (c < n) {
+        int e = h + c;
+        T v0 = U[e], v1 = U[nt + e], v2 = U[2 * nt + e];
+        push_ghosts_1d(U, nt, 0, c, n, h, bc, v0);
+        push_ghosts_1d(U, nt, 1, c, n, h, bc, v1);
+        push_ghosts_1d(U, nt, 2, c, n, h, bc, v2);
+        ms = (double)cell_speed_1d(v0, v1, v2, gamma, gm1);
+    }
+    ms = warp_max(ms);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = ms;
+    __syncthreads();
+    if (w == 0) {
+        double x = (l < T1 / 32) ? red[l] : 0.0;
+        x = warp_max(x);
+        if (l == 0) atomic_max_speed(&ctrl->maxs[p][0], x);
+    }
+}
+
+template <typename T>
+cudaError_t launch_1d_prepare_t(T* U, int n, int h, double gamma, int bc, StepCtrl* ctrl, int p, cudaStream_t st) {
+    int blocks = (n + T1 - 1) / T1;
+    k1d_prepare<T><<<blocks, T1, 0, st>>>(U, n, h, gamma, bc, ctrl, p);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_1d_step_t(T* U, T* U1, int n, int h, double dx, double gamma, int bc, const LoopParams& lp,
+                             StepCtrl* ctrl, int p, int which, cudaStream_t st, T* Uout) {
+    int blocks = (n + T1 - 1) / T1;
+    if (which & 1) k1d_stage<T, 1><<<blocks, T1, 0, st>>>(U, nullptr, U1, n, h, dx, gamma, bc, lp, ctrl, p);
+    if (which & 2) k1d_stage<T, 2><<<blocks, T1, 0, st>>>(U1, U, Uout ? Uout : U, n, h, dx, gamma, bc, lp, ctrl, p);
+    return cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace nestb

@@ -15,7 +15,7 @@ namespace nestb {
 
 struct Geo2D;
 
-// 1D (FP64, bit-exact with nest's OpenMP path)
+// 1D plain form (FP64, bit-exact with nest's OpenMP path)
 size_t resident_smem_bytes(int n, int h);
 cudaError_t launch_1d_resident(double* U, int n, int h, double dx, double gamma, int bc,
                                const LoopParams& lp, StepCtrl* ctrl, int p, cudaStream_t st);
@@ -26,6 +26,12 @@ cudaError_t launch_1d_prepare(double* U, int n, int h, double gamma, int bc, Ste
 cudaError_t launch_1d_step(double* U, double* U1, int n, int h, double dx, double gamma, int bc,
                            const LoopParams& lp, StepCtrl* ctrl, int p, int which, cudaStream_t st,
                            double* Uout = nullptr);
+// 1D FP32 form (tiled kernels only; time, dt and wave speeds in FP64).
+cudaError_t launch_1d_prepare_f32(float* U, int n, int h, double gamma, int bc, StepCtrl* ctrl, int p,
+                                  cudaStream_t st);
+cudaError_t launch_1d_step_f32(float* U, float* U1, int n, int h, double dx, double gamma, int bc,
+                               const LoopParams& lp, StepCtrl* ctrl, int p, int which, cudaStream_t st,
+                               float* Uout = nullptr);
 
 // 2D unsplit scheme.  `which`: 1 = stage 1, 2 = stage 2, 3 = both.
 cudaError_t launch_2d_prepare_f64(double* U, const Geo2D& g, StepCtrl* ctrl, int p, cudaStream_t st);

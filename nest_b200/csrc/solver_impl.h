@@ -74,7 +74,7 @@ struct nest_solver {
     std::map<nestb::rt::GraphKey, cudaGraphExec_t> graphs;
 
     bool resident() const {
-        return d.dim == 1 && !(d.flags & NEST_FLAG_NO_RESIDENT) &&
+        return d.dim == 1 && d.precision == NEST_F64 && !(d.flags & NEST_FLAG_NO_RESIDENT) &&
                nestb::resident_smem_bytes(d.nx, h) <= 220 * 1024;
     }
     nestb::Geo2D geo() const {

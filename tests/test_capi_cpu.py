@@ -43,7 +43,7 @@ def test_invalid_arguments_rejected_without_gpu():
         dict(dim=2, nx=8, ny=8, gamma=1.0),
         dict(dim=1, nx=16, halo=1),
         dict(dim=2, nx=8, ny=8, halo=3),
-        dict(dim=1, nx=16, precision=A.F32),
+        dict(dim=1, nx=16, precision=A.F32, flags=A.FLAG_TOTALS),
         dict(dim=2, nx=8, ny=8, dx=-1.0),
     ]
     for kw in bad:

@@ -90,3 +90,30 @@ def test_dts_record_then_freeze(gpu):
     steps = s2.run_to(1.0, 0.4)  # ends when the frozen sequence runs out
     assert steps == 40
     assert np.array_equal(s2.download()[:, 2:-2], a[:, 2:-2])
+
+
+@pytest.mark.parametrize("bc", [BC_OUTFLOW, BC_PERIODIC])
+def test_fp32_form_close_to_fp64(gpu, bc):
+    """The 1D FP32 form (tiled kernels, FP32 state and arithmetic, FP64 time
+    and dt) tracks the FP64 plain form on Sod to FP32 rounding level; ghost
+    cells follow the boundary rule."""
+    n = 1000
+    U = sod_ic_1d(n, 2)
+    a64 = gpu.Solver(1, n, bc=bc, flags=gpu.FLAG_NO_RESIDENT)
+    a64.upload(U)
+    k64 = a64.run_to(0.1, 0.4)
+    a32 = gpu.Solver(1, n, bc=bc, precision=gpu.F32)
+    a32.upload(U.astype(np.float32))
+    k32 = a32.run_to(0.1, 0.4)
+    assert abs(k32 - k64) <= 1
+    r64 = a64.download()[:, 2:-2]
+    got = a32.download()
+    r32 = got[:, 2:-2].astype(np.float64)
+    assert np.all(np.isfinite(r32))
+    scale = np.abs(r64).max(axis=1, keepdims=True)
+    assert (np.abs(r32 - r64) / scale).mean() < 1e-5
+    assert (np.abs(r32 - r64) / scale).max() < 2e-3
+    if bc == BC_OUTFLOW:
+        assert np.array_equal(got[:, 0], got[:, 2]) and np.array_equal(got[:, -1], got[:, -3])
+    else:
+        assert np.array_equal(got[:, 0], got[:, n]) and np.array_equal(got[:, -1], got[:, 3])

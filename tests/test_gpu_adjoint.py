@@ -227,3 +227,29 @@ def test_adjoint2d_fp32_vs_fp64(gpu):
     g64, g32 = out[gpu.F64], out[gpu.F32]
     rel = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
     assert rel < 1e-3, rel
+
+
+def test_adjoint1d_fp32_vs_fp64(gpu):
+    """1D adjoint of the FP32 form (FP32 forward, FP32 reverse stages, FP64
+    dt sequence) against the FP64 adjoint on the same loss: the L2 misfit
+    of the final density, gradient with respect to the initial state."""
+    from nest_b200.adjoint import Adjoint
+    n, nsteps = 512, 160
+    U0 = prim_to_cons_1d(*fourier_fields_1d(n, seed=1))
+    tgt = prim_to_cons_1d(*fourier_fields_1d(n, seed=2))[0, 2:-2]
+    grads = {}
+    for prec, dt in ((gpu.F64, np.float64), (gpu.F32, np.float32)):
+        flags = gpu.FLAG_NO_RESIDENT if prec == gpu.F64 else 0
+        s = gpu.Solver(1, n, bc=gpu.BC_PERIODIC, precision=prec, flags=flags)
+        s.upload(U0.astype(dt))
+        adj = Adjoint(s, nsteps, 1, 8)
+        adj.forward(0.4)
+        UT = s.download().astype(np.float64)
+        lamT = np.zeros_like(UT)
+        lamT[0, 2:-2] = (UT[0, 2:-2] - tgt) / n
+        grads[prec] = adj.backward(lamT.astype(dt)).astype(np.float64)[:, 2:-2]
+        adj.close()
+        s.close()
+    g64, g32 = grads[gpu.F64], grads[gpu.F32]
+    rel = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
+    assert np.all(np.isfinite(g32)) and rel < 1e-3, rel
