@@ -579,8 +579,8 @@ def bench_adjoint(args):
 
 
 def bench_sod1d(reps: int = 20):
-    """1D Sod: N = 1024, outflow, CFL 0.4 to t = 0.2, FP64 (one resident CTA
-    runs the whole loop).  Device time of run_to from the initial state;
+    """1D Sod: N = 1024, outflow, CFL 0.4 to t = 0.2, FP64 (one thread-block
+    cluster runs the whole loop).  Device time of run_to from the initial state;
     L1(rho) against the exact solution."""
     import torch
     import nest_b200 as nb
@@ -609,7 +609,8 @@ def bench_sod1d(reps: int = 20):
     s.close()
     return {"n": n, "bc": "outflow", "cfl": 0.4, "t_final": t, "steps": steps, "ms": m,
             "value": n * steps * 2 / (m * 1e-3), "unit": UNIT, "l1_rho_vs_exact": l1_rho_1d(rho, t),
-            "launches": 1, "dtype": "f64", "kernel": "k1d_resident (whole run in one CTA's shared memory)"}
+            "launches": 1, "dtype": "f64",
+            "kernel": "k1d_cluster (one thread-block cluster of 16 CTAs runs the whole loop in shared memory)"}
 
 
 def ke_v(U, nx, ny):
