@@ -66,19 +66,21 @@ __device__ __forceinline__ Q4 q_fma(F2 h, const Q4& s, const Q4& w) {
     return { fma2(h, s.a, w.a), fma2(h, s.b, w.b), fma2(h, s.c, w.c), fma2(h, s.d, w.d) };
 }
 
-// Per-lane asynchronous global -> shared copies (cp.async, 8 bytes: one
-// column pair of one variable).  A copy holds no registers while in flight.
-__device__ __forceinline__ void cp8(F2* smem_dst, const float* gsrc) {
+// Asynchronous global -> shared copy of 16 bytes (cp.async, L2 only): four
+// consecutive columns of one variable.  A copy holds no registers while in
+// flight.
+__device__ __forceinline__ void cp16(F2* smem_dst, const float* gsrc) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Shared-memory row rings of one warp: RING_U slots of the stage input and,
-// in stage 2, RING_N slots of U^n; a slot holds the lane's pair of the four
-// variables, [var][lane] so that a warp's 8-byte accesses are contiguous.
+// in stage 2, RING_N slots of U^n; a slot holds the warp's 64-column row
+// segment of the four variables, [var][64 columns], filled by 16-byte copies
+// (two per lane) and read as one column pair per lane.
 // LOOK: rows of the stage input in flight ahead of the row march (the row
 // issued at iteration i is consumed at iteration i + LOOK - 2); U^n runs
 // LOOK - 2 rows ahead.  Measured at 4096^2: LOOK 3 0.386 ms per step, 4 and
@@ -87,7 +89,7 @@ constexpr int LOOK = 3;
 constexpr int RING_U = 4, RING_N = 2;
 static_assert(RING_U >= LOOK + 1 && RING_N >= LOOK - 1, "ring too small for the lookahead");
 __host__ __device__ constexpr int ring_f2_per_warp(int stage) { return (RING_U + (stage == 2 ? RING_N : 0)) * 4 * 32; }
-extern __shared__ F2 x2_ring[];
+extern __shared__ __align__(16) F2 x2_ring[];
 
 // 1/x for a positive double x that is an FP32 value of at least 1e-10:
 // Newton-Raphson iteration y <- y + y (1 - x y), which doubles the number of
@@ -267,17 +269,23 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
     // into registers one row ahead, the update's re-read of its own row from
     // L1) ncu measured a 10 % L1 hit rate on that re-read and long-scoreboard
     // waits as the top stall, at 0.434 ms per 4096^2 step against 0.386.
-    F2* const ring = x2_ring + threadIdx.y * ring_f2_per_warp(STAGE) + lane;
-    auto stage_row = [&](int i) {
-        const float* q = Ui + (long long)(min(i, last_row) + 2) * pitch + coff;
-        F2* d = ring + (i & (RING_U - 1)) * 128;
-        cp8(d, q); cp8(d + 32, q + vs); cp8(d + 64, q + 2 * vs); cp8(d + 96, q + 3 * vs);
+    F2* const ringw = x2_ring + threadIdx.y * ring_f2_per_warp(STAGE);  // this warp's rings
+    F2* const ring = ringw + lane;                                       // this lane's column pair
+    // 16-byte chunk copies: lane l moves column chunk l & 15 (columns
+    // j0 - 2 + 4 (l & 15) .. + 3) of variables l >> 4 and (l >> 4) + 2.  Chunk
+    // starts are 16-byte aligned (j0 = 60 strip, pitch a multiple of 32); a
+    // chunk past the row end re-reads the row's last four columns, which feed
+    // only discarded lanes.
+    const int part = lane & 15, cvar = lane >> 4;
+    const long long cseg = view_offset(a) + min(j0 + 4 * part, pitch - 4) + (long long)cvar * vs;
+    const int cofs = cvar * 32 + 2 * part;  // F2 index of the chunk in a slot
+    auto stage_rows = [&](const float* base, int i, F2* slot) {
+        const float* q = base + (long long)(min(i, last_row) + 2) * pitch + cseg;
+        cp16(slot + cofs, q);
+        cp16(slot + cofs + 64, q + 2 * vs);
     };
-    auto stage_un = [&](int i) {
-        const float* q = Unp + (long long)(min(i, last_row) + 2) * pitch + coff;
-        F2* d = ring + RING_U * 128 + (i & (RING_N - 1)) * 128;
-        cp8(d, q); cp8(d + 32, q + vs); cp8(d + 64, q + 2 * vs); cp8(d + 96, q + 3 * vs);
-    };
+    auto stage_row = [&](int i) { stage_rows(Ui, i, ringw + (i & (RING_U - 1)) * 128); };
+    auto stage_un = [&](int i) { stage_rows(Unp, i, ringw + RING_U * 128 + (i & (RING_N - 1)) * 128); };
     auto ring_row = [&](int i, Q4& q) {
         const F2* d = ring + (i & (RING_U - 1)) * 128;
         q.a = d[0]; q.b = d[32]; q.c = d[64]; q.d = d[96];
