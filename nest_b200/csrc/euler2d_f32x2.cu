@@ -5,9 +5,11 @@
 // the FFMA2/FADD2/FMUL2 instructions of sm_100 (one issue slot per two
 // cells).  A warp covers 64 columns j0-2 .. j0+61 and writes 60 of them
 // (lanes 1..30; lanes 0 and 31 only feed their neighbours), marching down a
-// tile of rows with a three-row register window exactly like the scalar
-// kernel in euler2d_kernels.cuh.  Per lane and row:
-//   * 64-bit loads/stores of the (a, b) pair of each variable,
+// tile of rows with a three-row register window like the scalar kernel in
+// euler2d_kernels.cuh.  Per lane and row:
+//   * input rows staged through shared memory by 16-byte cp.async copies
+//     (see x2_body), read back and stored as the lane's 64-bit (a, b) pair of
+//     each variable,
 //   * x-faces: one packed HLLE for the faces under columns a and b,
 //   * y-faces: one packed HLLE for the faces a|b and b|a' (a' = next lane's
 //     first column), with 2 + 1 + 1 shuffles per variable.
@@ -16,31 +18,13 @@
 // weights (hlle2 below).
 // Compiled with -use_fast_math: reciprocal and rsqrt are single MUFU ops.
 #include "euler2d_kernels.cuh"
+#include "f2ops.cuh"
 #include "kernels.h"
 
 namespace nestb {
 namespace {
 
 constexpr int STRIP2 = 60;  // output columns per warp
-
-
-
-using F2 = float2;
-
-__device__ __forceinline__ F2 sp(float a) { return make_float2(a, a); }
-__device__ __forceinline__ F2 add2(F2 a, F2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ F2 sub2(F2 a, F2 b) {
-    F2 o;
-    asm("{\n\t.reg .b64 ta, tb, tr;\n\tmov.b64 ta, {%2, %3};\n\tmov.b64 tb, {%4, %5};\n\t"
-        "sub.rn.f32x2 tr, ta, tb;\n\tmov.b64 {%0, %1}, tr;\n\t}"
-        : "=f"(o.x), "=f"(o.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return o;
-}
-__device__ __forceinline__ F2 mul2(F2 a, F2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ F2 rcp2(F2 a) { return make_float2(__fdividef(1.f, a.x), __fdividef(1.f, a.y)); }
-__device__ __forceinline__ F2 rsq2(F2 a) { return make_float2(rsqrtf(a.x), rsqrtf(a.y)); }
-__device__ __forceinline__ F2 max2(F2 a, float b) { return make_float2(fmaxf(a.x, b), fmaxf(a.y, b)); }
 
 // nest's minmod (euler1d.hpp:112-115) in three ALU operations:
 // min.xorsign.abs gives min(|a|, |b|) carrying the sign sign(a) xor sign(b),
