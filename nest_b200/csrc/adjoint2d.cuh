@@ -36,8 +36,7 @@ struct Adj4 { T r, n, t, p; };
 
 // Reverse sweep of hlle4 (normal n, transverse t) for one face.
 template <typename T>
-__device__ __forceinline__ void hlle4_adj(T gamma, T gm1, Adj4<T> L, Adj4<T> R, const T fb[4], T wl[4], T wr[4]) {
-    const T igm1 = T(1) / gm1;
+__device__ __forceinline__ void hlle4_adj(T gamma, T igm1, Adj4<T> L, Adj4<T> R, const T fb[4], T wl[4], T wr[4]) {
     T cL = sqrt(gamma * L.p / L.r), cR = sqrt(gamma * R.p / R.r);
     T EL = L.p * igm1 + T(0.5) * L.r * (L.n * L.n + L.t * L.t);
     T ER = R.p * igm1 + T(0.5) * R.r * (R.n * R.n + R.t * R.t);
@@ -79,10 +78,10 @@ __device__ __forceinline__ void hlle4_adj(T gamma, T gm1, Adj4<T> L, Adj4<T> R, 
         rb += ub_[0]; rb += ub_[1] * S.n; nb += ub_[1] * S.r;
         rb += ub_[2] * S.t; tb += ub_[2] * S.r; Eb += ub_[3];
         pb += Eb * igm1; rb += Eb * T(0.5) * (S.n * S.n + S.t * S.t); nb += Eb * S.r * S.n; tb += Eb * S.r * S.t;
-        if (c > T(0)) {  // c = sqrt(g p / r): dc/dp = g / (2 r c), dc/dr = -c / (2 r)
-            const T i2r = T(0.5) / S.r;
-            pb += cb * gamma * i2r / c;
-            rb -= cb * c * i2r;
+        if (c > T(0)) {  // c = sqrt(g p / r): dc/dp = g / (2 r c), dc/dr = -c / (2 r) = -c^2 / (2 r c)
+            const T q = T(0.5) / (S.r * c);
+            pb += cb * gamma * q;
+            rb -= cb * (c * c) * q;
         }
         wo[0] += rb; wo[1] += nb; wo[2] += tb; wo[3] += pb;
     };
@@ -144,7 +143,7 @@ __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lo
     const int tid = threadIdx.x;
     const int i0 = blockIdx.y * ATX, j0 = blockIdx.x * ATY;
     const long long vs = g.vstride;
-    const T gamma = (T)g.gamma, gm1 = (T)(g.gamma - 1.0);
+    const T gamma = (T)g.gamma, gm1 = (T)(g.gamma - 1.0), igm1 = (T)(1.0 / (g.gamma - 1.0));
     // periodic wrap; tile cells beyond the domain (only read by threads that
     // return early) may lie more than one period away on small domains
     auto wrapi = [&](int i) {
@@ -212,7 +211,7 @@ __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lo
         T fb[4], wl[4] = {0, 0, 0, 0}, wr[4] = {0, 0, 0, 0};
         for (int k = 0; k < 4; ++k) fb[k] = lx * (Lo[k][f + 1][b + 2] - Lo[k][f][b + 2]);
         // components (rho, mu, mv, E) -> (rho, normal, transverse, E): x normal = u
-        hlle4_adj(gamma, gm1, L, R, fb, wl, wr);
+        hlle4_adj(gamma, igm1, L, R, fb, wl, wr);
         for (int k = 0; k < 4; ++k) { XL[k][f][b] = wl[k]; XR[k][f][b] = wr[k]; }
     }
     if (tid < ATX * (ATY + 3)) {
@@ -226,7 +225,7 @@ __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lo
         T fb[4] = { ly * (Lo[0][a + 2][f + 1] - Lo[0][a + 2][f]), ly * (Lo[2][a + 2][f + 1] - Lo[2][a + 2][f]),
                     ly * (Lo[1][a + 2][f + 1] - Lo[1][a + 2][f]), ly * (Lo[3][a + 2][f + 1] - Lo[3][a + 2][f]) };
         T wl[4] = {0, 0, 0, 0}, wr[4] = {0, 0, 0, 0};
-        hlle4_adj(gamma, gm1, L, R, fb, wl, wr);
+        hlle4_adj(gamma, igm1, L, R, fb, wl, wr);
         // back to (rho, u, v, p)
         YL[0][a][f] = wl[0]; YL[1][a][f] = wl[2]; YL[2][a][f] = wl[1]; YL[3][a][f] = wl[3];
         YR[0][a][f] = wr[0]; YR[1][a][f] = wr[2]; YR[2][a][f] = wr[1]; YR[3][a][f] = wr[3];

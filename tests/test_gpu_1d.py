@@ -27,8 +27,11 @@ def test_dropin_matches_reference_test(gpu):
     assert np.array_equal(got[:, 2:-2], want[:, 2:-2])
 
 
+# 257 / 1000 cells split unevenly over the resident solver's 16-CTA cluster
+# (last chunk 2 / 55 cells)
 @pytest.mark.parametrize("n,bc,cfl,tf", [(1024, BC_OUTFLOW, 0.4, 0.2), (1024, BC_PERIODIC, 0.4, 0.2),
-                                         (97, BC_OUTFLOW, 0.8, 0.1), (2300, BC_PERIODIC, 0.4, 0.05)])
+                                         (97, BC_OUTFLOW, 0.8, 0.1), (2300, BC_PERIODIC, 0.4, 0.05),
+                                         (257, BC_PERIODIC, 0.5, 0.1), (1000, BC_OUTFLOW, 0.4, 0.1)])
 @pytest.mark.parametrize("resident", [True, False])
 def test_run_to_matches_oracle(gpu, oracle, n, bc, cfl, tf, resident):
     U = sod_ic_1d(n)
