@@ -40,6 +40,7 @@ UNITS = {
     "exchange.cu": [],
     "adjoint2d.cu": [],
     "adjoint2d_f32.cu": ["-use_fast_math"],
+    "adjoint2d_f32x2.cu": ["-use_fast_math"],
     "datio.cpp": ["-x", "cu", "-Xcompiler", "-ffp-contract=off"],
 }
 

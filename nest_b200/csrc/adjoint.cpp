@@ -19,6 +19,7 @@
 // (Heun: U^{n+1} = 1/2 (U^n + S(S(U^n)))).
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <memory>
 #include <new>
 #include <vector>
@@ -90,7 +91,14 @@ struct Stepper1D : Stepper {
 struct Stepper2D : Stepper {
     nest_solver* s;
     StepCtrl* ctrl;
-    Stepper2D(nest_solver* s_, StepCtrl* c) : s(s_), ctrl(c) {}
+    // NEST_ADJOINT2D_TILE=1 in the environment when the adjoint is created
+    // selects the FP32 tile kernel for every ny (a diagnostic: both FP32
+    // kernels can then be compared on one trajectory)
+    bool tile32 = false;
+    Stepper2D(nest_solver* s_, StepCtrl* c) : s(s_), ctrl(c) {
+        const char* e = std::getenv("NEST_ADJOINT2D_TILE");
+        tile32 = e && e[0] == '1';
+    }
     cudaError_t stage(int which, void* Un, void* U1, void* Uout, const LoopParams& lp, int p) override {
         if (s->d.precision == NEST_F64)
             return launch_2d_step_f64((double*)Un, (double*)U1, s->geo(), lp, ctrl, nullptr, p, s->tx, s->warps, which,
@@ -107,11 +115,18 @@ struct Stepper2D : Stepper {
                 e = launch_2d_adjoint_stage_f64((const double*)Un, (const double*)tmp, (const double*)lam,
                                                 (double*)lam_new, s->geo(), dtp, 1.0, 0.5, s->st);
         } else {
-            e = launch_2d_adjoint_stage_f32((const float*)U1, (const float*)lam, nullptr, (float*)tmp, s->geo(), dtp,
-                                            0.5, 0.0, s->st);
+            // packed row march; the tile kernel for an odd ny, which the packed
+            // kernel does not take
+            auto st32 = [&](const float* U, const float* Lo, const float* Ex, float* Li, double al, double be) {
+                cudaError_t r = cudaErrorNotSupported;
+                if (!tile32) r = launch_2d_adjoint_stage_f32x2(U, Lo, Ex, Li, s->geo(), dtp, al, be, s->st);
+                if (r == cudaErrorNotSupported)
+                    r = launch_2d_adjoint_stage_f32(U, Lo, Ex, Li, s->geo(), dtp, al, be, s->st);
+                return r;
+            };
+            e = st32((const float*)U1, (const float*)lam, nullptr, (float*)tmp, 0.5, 0.0);
             if (e == cudaSuccess)
-                e = launch_2d_adjoint_stage_f32((const float*)Un, (const float*)tmp, (const float*)lam,
-                                                (float*)lam_new, s->geo(), dtp, 1.0, 0.5, s->st);
+                e = st32((const float*)Un, (const float*)tmp, (const float*)lam, (float*)lam_new, 1.0, 0.5);
         }
         return e;
     }

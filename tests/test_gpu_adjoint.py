@@ -229,6 +229,31 @@ def test_adjoint2d_fp32_vs_fp64(gpu):
     assert rel < 1e-3, rel
 
 
+@pytest.mark.parametrize("nx,ny", [(12, 10), (48, 40), (130, 118), (70, 64), (200, 232)])
+def test_adjoint2d_fp32_row_march(gpu, nx, ny, monkeypatch):
+    """The FP32 form's adjoint stage, a packed row march with one strip of
+    56 columns per warp (several strips, ragged strips and row segments,
+    domains narrower than a strip), against the FP32 tile kernel on the same
+    FP32 trajectory (NEST_ADJOINT2D_TILE=1): smooth fields, 6 steps, random
+    final adjoint.  Both reverse the same discrete map; they differ by FP32
+    rounding of the reverse sweep (relative L2 about 1e-6).  Against the FP64
+    adjoint the difference is larger (1e-3 at 130 x 118): FP32 rounding of
+    the trajectory moves a few near-ties of |d1| and |d2| to the other minmod
+    branch, which changes that cell's derivative by order one."""
+    lam = {}
+    for key, tile in (("march", "0"), ("tile", "1")):
+        monkeypatch.setenv("NEST_ADJOINT2D_TILE", tile)
+        U0, s, adj = adjoint2d_case(gpu, nx, ny, 6, gpu.F32, seed=6, smooth=True)
+        UT = s.download()
+        w = np.random.default_rng(9).standard_normal((4, nx, ny))
+        lamT = np.zeros(UT.shape, dtype=np.float32)
+        lamT[:, 2:-2, 2:-2] = w
+        lam[key] = adj.backward(lamT).astype(np.float64)[:, 2:-2, 2:-2]
+    assert np.all(np.isfinite(lam["march"]))
+    rel = np.linalg.norm(lam["march"] - lam["tile"]) / np.linalg.norm(lam["tile"])
+    assert rel < 1e-4, rel
+
+
 def test_adjoint1d_fp32_vs_fp64(gpu):
     """1D adjoint of the FP32 form (FP32 forward, FP32 reverse stages, FP64
     dt sequence) against the FP64 adjoint on the same loss: the L2 misfit
