@@ -34,8 +34,19 @@
 namespace nestb {
 namespace {
 
-constexpr int ASTRIP = 56;  // output columns per warp
-constexpr int AWARPS = 4;   // warps per CTA (strips side by side)
+// Launch shape and register budget, measured on the 2048^2 FP32 KH adjoint
+// (200 steps, backward ms): 2 warps per CTA at 200 registers (198 used, no
+// spills, 10 warps per SM) 75.7; 2 or 4 warps at 168 (16 bytes spilled, 12
+// warps per SM) 76.1 / 77.2; 144 registers 84.3; 128 registers 94.7; the
+// march unrolled by 2 / 3 76.4 / 84.0.
+#ifndef NEST_ADJX2_WARPS
+#define NEST_ADJX2_WARPS 2
+#define NEST_ADJX2_REGS 200
+#define NEST_ADJX2_UNROLL 1
+#endif
+constexpr int ASTRIP = 56;                // output columns per warp
+constexpr int AWARPS = NEST_ADJX2_WARPS;  // warps per CTA (strips side by side)
+constexpr int AUNROLL = NEST_ADJX2_UNROLL;
 // ring slots per warp: conserved rows (2), Lout rows (4), Extra rows (2),
 // each [4 variables][32 lanes] float2
 constexpr int RU = 2, RL = 4, RE = 2;
@@ -177,9 +188,7 @@ struct AdjX2Args {
     int seg_rows;  // rows per warp segment
 };
 
-// 168 registers: 12 warps per SM with 16 bytes of spills (the unbounded
-// kernel takes 196 registers, 8 warps per SM; 128 spills 380 bytes).
-__global__ void __maxnreg__(168) k2d_adjoint_x2(AdjX2Args A) {
+__global__ void __maxnreg__(NEST_ADJX2_REGS) k2d_adjoint_x2(AdjX2Args A) {
     const Geo2D& g = A.g;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int strip = blockIdx.x * AWARPS + warp;
@@ -260,7 +269,7 @@ __global__ void __maxnreg__(168) k2d_adjoint_x2(AdjX2Args A) {
     Q4 Bm = { z, z, z, z }, B0 = { z, z, z, z };  // primitive adjoints of rows a-1, a
     Q4 Sp = { z, z, z, z };                       // x-slope adjoint of row a so far
 
-#pragma unroll 1
+#pragma unroll AUNROLL
     for (int a = r0 - 2; a <= r0 + rows; ++a) {
         issue(A.U, a + 3, ringU + ((a + 3) & (RU - 1)) * 128);
         issue(A.Lout, a + 2, ringL + ((a + 2) & (RL - 1)) * 128);
