@@ -87,10 +87,10 @@ __device__ void hlle1d_adj(T gamma, T gm1, St3<T> L, St3<T> R, const T fb[3], T 
         // E = p / (g-1) + 0.5 r u^2
         pb += Eb * igm1; rb += Eb * T(0.5) * S.u * S.u; ub += Eb * S.r * S.u;
         // c = sqrt(g p / r): dc/dp = g / (2 r c), dc/dr = -c / (2 r)
-        if (c > T(0)) {
-            const T i2r = T(0.5) / S.r;
-            pb += cbar * gamma * i2r / c;
-            rb -= cbar * c * i2r;
+        if (c > T(0)) {  // 1 / (2 r c) once: dc/dr = -c^2 / (2 r c)
+            const T q = T(0.5) / (S.r * c);
+            pb += cbar * gamma * q;
+            rb -= cbar * (c * c) * q;
         }
         wo[0] += rb; wo[1] += ub; wo[2] += pb;
     };
