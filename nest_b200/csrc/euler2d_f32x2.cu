@@ -135,15 +135,20 @@ __device__ __forceinline__ Q4 prim2(const Q4& U, float gm1) {
 __device__ __forceinline__ void hlle2(float gamma, float igm1, F2 scale,
                                       F2 rL, F2 nL, F2 tL, F2 pL, F2 rR, F2 nR, F2 tR, F2 pR,
                                       F2& f0, F2& f1, F2& f2, F2& f3) {
-    F2 g = sp(gamma), h = sp(0.5f);
+    F2 g = sp(gamma), h = sp(0.5f), tiny = sp(1e-37f);
     F2 gpL = mul2(g, pL), gpR = mul2(g, pR);
-    F2 cL = mul2(gpL, rsq2(max2(mul2(gpL, rL), 1e-37f)));
-    F2 cR = mul2(gpR, rsq2(max2(mul2(gpR, rR), 1e-37f)));
-    // nsl = -min(S_L, 0) = max(c_L - u_L, c_R - u_R, 0), sr = max(S_R, 0)
+    // c = g p / sqrt(g p rho + 1e-37): the added 1e-37 keeps p = 0 finite
+    // (c = 0) and is below the rounding of any state with p, rho >= 1e-15
+    F2 cL = mul2(gpL, rsq2(fma2(gpL, rL, tiny)));
+    F2 cR = mul2(gpR, rsq2(fma2(gpR, rR, tiny)));
+    // nsl = -min(S_L, 0) = max(c_L - u_L, c_R - u_R, 0), sr = max(S_R, 0);
+    // nsl is floored at 1e-30 instead of 0, which keeps sr + nsl > 0 (a
+    // vacuum at rest) and gives the supersonic-right flux an extra weight
+    // 1e-30 / sr on F_R - sr U_R, far below the rounding of F_L
     F2 aL = sub2(cL, nL), aR = sub2(cR, nR), bL = add2(nL, cL), bR = add2(nR, cR);
-    F2 nsl = make_float2(max3f(aL.x, aR.x, 0.f), max3f(aL.y, aR.y, 0.f));
+    F2 nsl = make_float2(max3f(aL.x, aR.x, 1e-30f), max3f(aL.y, aR.y, 1e-30f));
     F2 sr = make_float2(max3f(bL.x, bR.x, 0.f), max3f(bL.y, bR.y, 0.f));
-    F2 inv = mul2(scale, rcp2(max2(add2(sr, nsl), 1e-30f)));
+    F2 inv = mul2(scale, rcp2(add2(sr, nsl)));
     F2 A = mul2(sr, inv);   //  scale sr / (sr - sl)
     F2 B = mul2(nsl, inv);  // -scale sl / (sr - sl)
     F2 dL = add2(nL, nsl), dR = sub2(nR, sr);
