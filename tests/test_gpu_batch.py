@@ -88,3 +88,28 @@ def test_batch_info_and_uneven_sizes(gpu):
     assert len(np.unique(np.round(t, 12))) > 1
     for p in (0, 7, 23):
         assert np.all(np.isfinite(b.download(p)))
+
+
+@pytest.mark.parametrize("tiling", [(8, 2, 1), (8, 4, 1), (8, 4, 2)])
+def test_batch_fp32_multiwarp_matches_single(gpu, tiling):
+    """Persistent FP32 batch with several warps per block and several work
+    items per warp (each warp stages the rows of one item after another
+    through the same shared-memory ring slots) against the single-domain
+    FP32 solver, bit for bit per problem."""
+    sizes = [(256, 256), (192, 320), (128, 200), (300, 128)] * 6
+    nx = [a for a, _ in sizes]
+    ny = [c for _, c in sizes]
+    flags = gpu.FLAG_TOTALS | gpu.FLAG_REPAIR
+    b = gpu.Batch(nx, ny, precision=gpu.F32, flags=flags)
+    b.set_tiling(*tiling)
+    ics = [kelvin_helmholtz(a, c, seed=1 + p).astype(np.float32) for p, (a, c) in enumerate(sizes)]
+    for p, U in enumerate(ics):
+        b.upload(p, U)
+    b.step(30, 0.4)
+    _, items, blocks = b.info()
+    assert items > 2 * blocks * tiling[1]  # several items per warp
+    for p, (a, c) in enumerate(sizes):
+        s = gpu.Solver(2, a, c, bc=gpu.BC_PERIODIC, precision=gpu.F32, flags=flags)
+        s.upload(ics[p])
+        s.step(30, 0.4)
+        assert np.array_equal(b.download(p)[:, 2:-2, 2:-2], s.download()[:, 2:-2, 2:-2]), p
