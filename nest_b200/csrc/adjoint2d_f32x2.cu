@@ -30,6 +30,7 @@
 #include "kernels.h"
 
 #include <algorithm>
+#include <mutex>
 
 namespace nestb {
 namespace {
@@ -412,17 +413,34 @@ cudaError_t launch_2d_adjoint_stage_f32x2(const float* U, const float* Lout, con
                                           cudaStream_t st) {
     if ((g.ny & 1) || g.pitch % 2 != 0) return cudaErrorNotSupported;
     const size_t smem = sizeof(F2) * RING_F2 * AWARPS;
-    int dev = 0, sms = 0, per_sm = 0;
+    // per-device launch facts, looked up once (SM count, resident CTAs)
+    constexpr int MAXDEV = 64;
+    static std::mutex mu;
+    static int dev_sms[MAXDEV] = {}, dev_per_sm[MAXDEV] = {};
+    int dev = 0;
     cudaError_t e;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(k2d_adjoint_x2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
-        cudaSuccess)
-        return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2d_adjoint_x2, 32 * AWARPS, smem)) !=
-        cudaSuccess)
-        return e;
-    if (per_sm < 1) per_sm = 1;
+    int sms = 0, per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev < MAXDEV && dev_sms[dev] > 0) {
+            sms = dev_sms[dev];
+            per_sm = dev_per_sm[dev];
+        } else {
+            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+            if ((e = cudaFuncSetAttribute(k2d_adjoint_x2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+                cudaSuccess)
+                return e;
+            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k2d_adjoint_x2, 32 * AWARPS, smem)) !=
+                cudaSuccess)
+                return e;
+            if (per_sm < 1) per_sm = 1;
+            if (dev < MAXDEV) {
+                dev_sms[dev] = sms;
+                dev_per_sm[dev] = per_sm;
+            }
+        }
+    }
     const int strips = (g.ny + ASTRIP - 1) / ASTRIP;
     const int cx = (strips + AWARPS - 1) / AWARPS;
     // enough row segments for one wave of resident warps, at least 16 rows each

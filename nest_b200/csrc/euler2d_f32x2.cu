@@ -306,10 +306,13 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
 
     float smx = 0.f, smy = 0.f;
     double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
-    // Not unrolled: at 4096^2 an unroll of 2 (which removes the window
-    // rotation's register copies) gained 3 % in the plain kernels but lost
-    // 2 % in the repair + totals ones; 3 and 4 lost 12-25 %.
-#pragma unroll 1
+    // Unrolled by 2 in the plain kernels only (the unroll removes part of the
+    // window rotation's register copies).  Measured at 4096^2 (ms per step,
+    // stage 1 + stage 2): plain 0.3823 -> 0.3627 with the unroll; with
+    // repair + totals 0.4086 -> 0.4211 (stage 2 +5 %, near the 128-register
+    // budget); unrolls of 3 and 4 lost 12-25 %.
+    constexpr int kUnroll = (!REPAIR && !TOT) ? 2 : 1;
+#pragma unroll kUnroll
     for (int k = 0; k < rows; ++k) {
         const int i = i0 + k;
         Q4 cur;
