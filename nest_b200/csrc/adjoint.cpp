@@ -92,12 +92,12 @@ struct Stepper2D : Stepper {
     nest_solver* s;
     StepCtrl* ctrl;
     // NEST_ADJOINT2D_TILE=1 in the environment when the adjoint is created
-    // selects the FP32 tile kernel for every ny (a diagnostic: both FP32
-    // kernels can then be compared on one trajectory)
-    bool tile32 = false;
+    // selects the tile kernels instead of the row marches (a diagnostic: both
+    // forms can then be compared on one trajectory)
+    bool tile = false;
     Stepper2D(nest_solver* s_, StepCtrl* c) : s(s_), ctrl(c) {
         const char* e = std::getenv("NEST_ADJOINT2D_TILE");
-        tile32 = e && e[0] == '1';
+        tile = e && e[0] == '1';
     }
     cudaError_t stage(int which, void* Un, void* U1, void* Uout, const LoopParams& lp, int p) override {
         if (s->d.precision == NEST_F64)
@@ -109,17 +109,19 @@ struct Stepper2D : Stepper {
     cudaError_t adjoint_step(void* Un, void* U1, const double* dtp, void* lam, void* lam_new, void* tmp) override {
         cudaError_t e;
         if (s->d.precision == NEST_F64) {
-            e = launch_2d_adjoint_stage_f64((const double*)U1, (const double*)lam, nullptr, (double*)tmp, s->geo(), dtp,
-                                            0.5, 0.0, s->st);
+            auto st64 = [&](const double* U, const double* Lo, const double* Ex, double* Li, double al, double be) {
+                return tile ? launch_2d_adjoint_stage_f64(U, Lo, Ex, Li, s->geo(), dtp, al, be, s->st)
+                            : launch_2d_adjoint_stage_f64rm(U, Lo, Ex, Li, s->geo(), dtp, al, be, s->st);
+            };
+            e = st64((const double*)U1, (const double*)lam, nullptr, (double*)tmp, 0.5, 0.0);
             if (e == cudaSuccess)
-                e = launch_2d_adjoint_stage_f64((const double*)Un, (const double*)tmp, (const double*)lam,
-                                                (double*)lam_new, s->geo(), dtp, 1.0, 0.5, s->st);
+                e = st64((const double*)Un, (const double*)tmp, (const double*)lam, (double*)lam_new, 1.0, 0.5);
         } else {
             // packed row march; the tile kernel for an odd ny, which the packed
             // kernel does not take
             auto st32 = [&](const float* U, const float* Lo, const float* Ex, float* Li, double al, double be) {
                 cudaError_t r = cudaErrorNotSupported;
-                if (!tile32) r = launch_2d_adjoint_stage_f32x2(U, Lo, Ex, Li, s->geo(), dtp, al, be, s->st);
+                if (!tile) r = launch_2d_adjoint_stage_f32x2(U, Lo, Ex, Li, s->geo(), dtp, al, be, s->st);
                 if (r == cudaErrorNotSupported)
                     r = launch_2d_adjoint_stage_f32(U, Lo, Ex, Li, s->geo(), dtp, al, be, s->st);
                 return r;

@@ -60,6 +60,10 @@ cudaError_t launch_2d_adjoint_stage_f64(const double* U, const double* Lout, con
 cudaError_t launch_2d_adjoint_stage_f32(const float* U, const float* Lout, const float* Extra, float* Lin,
                                         const Geo2D& g, const double* dtp, double alpha, double beta,
                                         cudaStream_t st);
+// Row-march form of the FP64 stage (one column per lane, any ny).
+cudaError_t launch_2d_adjoint_stage_f64rm(const double* U, const double* Lout, const double* Extra, double* Lin,
+                                          const Geo2D& g, const double* dtp, double alpha, double beta,
+                                          cudaStream_t st);
 // Packed FP32x2 row-march form of the same stage; cudaErrorNotSupported
 // (nothing launched) for an odd ny.
 cudaError_t launch_2d_adjoint_stage_f32x2(const float* U, const float* Lout, const float* Extra, float* Lin,

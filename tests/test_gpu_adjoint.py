@@ -254,6 +254,26 @@ def test_adjoint2d_fp32_row_march(gpu, nx, ny, monkeypatch):
     assert rel < 1e-4, rel
 
 
+@pytest.mark.parametrize("nx,ny", [(12, 10), (48, 40), (130, 118), (64, 63), (31, 77)])
+def test_adjoint2d_fp64_row_march(gpu, nx, ny, monkeypatch):
+    """The FP64 row-march adjoint stage (one column per lane, strips of 26
+    columns; odd and narrow domains) against the FP64 tile kernel on the
+    same trajectory, smooth fields: same map, same subgradients, FP64
+    rounding of the reverse sweep only.  The exact-tangent and
+    finite-difference tests above run the row march on KH and smooth data."""
+    lam = {}
+    for key, tile in (("march", "0"), ("tile", "1")):
+        monkeypatch.setenv("NEST_ADJOINT2D_TILE", tile)
+        U0, s, adj = adjoint2d_case(gpu, nx, ny, 5, gpu.F64, seed=7, smooth=True)
+        UT = s.download()
+        w = np.random.default_rng(11).standard_normal((4, nx, ny))
+        lamT = np.zeros(UT.shape)
+        lamT[:, 2:-2, 2:-2] = w
+        lam[key] = adj.backward(lamT)[:, 2:-2, 2:-2]
+    rel = np.linalg.norm(lam["march"] - lam["tile"]) / np.linalg.norm(lam["tile"])
+    assert rel < 1e-12, rel
+
+
 def test_adjoint1d_fp32_vs_fp64(gpu):
     """1D adjoint of the FP32 form (FP32 forward, FP32 reverse stages, FP64
     dt sequence) against the FP64 adjoint on the same loss: the L2 misfit
