@@ -24,8 +24,16 @@
 namespace nestb {
 namespace {
 
-constexpr int DSTRIP = 26;  // output columns per warp
-constexpr int DWARPS = 2;   // warps per CTA
+// Launch shape and register budget, measured on the 2048^2 FP64 KH adjoint
+// (300 steps, backward ms): 2 warps per CTA at 168 registers (12 warps per
+// SM, no spills) 570; unbounded (176 registers, 10 warps per SM) 611 with 1,
+// 2 or 4 warps per CTA; 152 / 128 registers (spills) 591 / 592.
+#ifndef NEST_ADJ64_WARPS
+#define NEST_ADJ64_WARPS 2
+#define NEST_ADJ64_REGS 168
+#endif
+constexpr int DSTRIP = 26;                // output columns per warp
+constexpr int DWARPS = NEST_ADJ64_WARPS;  // warps per CTA
 constexpr int DRU = 2, DRL = 4, DRE = 2;  // ring slots: conserved rows, Lout rows, Extra rows
 constexpr int DRING = (DRU + DRL + DRE) * 4 * 32;  // doubles per warp
 extern __shared__ __align__(16) double adj64_ring[];
@@ -130,7 +138,12 @@ struct AdjD64Args {
     int seg_rows;
 };
 
-__global__ void __launch_bounds__(32 * DWARPS) k2d_adjoint_rm64(AdjD64Args A) {
+#if NEST_ADJ64_REGS > 0
+#define NEST_ADJ64_ATTR __maxnreg__(NEST_ADJ64_REGS)
+#else
+#define NEST_ADJ64_ATTR __launch_bounds__(32 * DWARPS)
+#endif
+__global__ void NEST_ADJ64_ATTR k2d_adjoint_rm64(AdjD64Args A) {
     const Geo2D& g = A.g;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int strip = blockIdx.x * DWARPS + warp;
