@@ -36,6 +36,12 @@ cudaError_t launch_1d_adjoint_stage(const double* U, const double* Lout, const d
 cudaError_t launch_1d_adjoint_stage_f32(const float* U, const float* Lout, const float* Extra, float* Lin, int n,
                                         int h, const double* dtp, double dx, double gamma, double alpha, double beta,
                                         cudaStream_t st);
+// Both reverse stages of one Heun step in one launch (the intermediate adjoint
+// stays in shared memory).
+cudaError_t launch_1d_adjoint_step(const double* Un, const double* U1, const double* lam, double* lam_new, int n,
+                                   int h, const double* dtp, double dx, double gamma, cudaStream_t st);
+cudaError_t launch_1d_adjoint_step_f32(const float* Un, const float* U1, const float* lam, float* lam_new, int n,
+                                       int h, const double* dtp, double dx, double gamma, cudaStream_t st);
 }
 
 namespace {
@@ -69,20 +75,13 @@ struct Stepper1D : Stepper {
         return launch_1d_step((double*)Un, (double*)U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp, ctrl, p,
                               which, s->st, (double*)Uout);
     }
-    cudaError_t adjoint_step(void* Un, void* U1, const double* dtp, void* lam, void* lam_new, void* tmp) override {
+    cudaError_t adjoint_step(void* Un, void* U1, const double* dtp, void* lam, void* lam_new, void*) override {
         const int n = s->d.nx, h = s->h;
-        if (s->d.precision == NEST_F32) {
-            cudaError_t e = launch_1d_adjoint_stage_f32((const float*)U1, (const float*)lam, nullptr, (float*)tmp, n,
-                                                        h, dtp, s->d.dx, s->d.gamma, 0.5, 0.0, s->st);
-            if (e != cudaSuccess) return e;
-            return launch_1d_adjoint_stage_f32((const float*)Un, (const float*)tmp, (const float*)lam,
-                                               (float*)lam_new, n, h, dtp, s->d.dx, s->d.gamma, 1.0, 0.5, s->st);
-        }
-        cudaError_t e = launch_1d_adjoint_stage((const double*)U1, (const double*)lam, nullptr, (double*)tmp, n, h,
-                                                dtp, s->d.dx, s->d.gamma, 0.5, 0.0, s->st);
-        if (e != cudaSuccess) return e;
-        return launch_1d_adjoint_stage((const double*)Un, (const double*)tmp, (const double*)lam,
-                                       (double*)lam_new, n, h, dtp, s->d.dx, s->d.gamma, 1.0, 0.5, s->st);
+        if (s->d.precision == NEST_F32)
+            return launch_1d_adjoint_step_f32((const float*)Un, (const float*)U1, (const float*)lam, (float*)lam_new,
+                                              n, h, dtp, s->d.dx, s->d.gamma, s->st);
+        return launch_1d_adjoint_step((const double*)Un, (const double*)U1, (const double*)lam, (double*)lam_new, n,
+                                      h, dtp, s->d.dx, s->d.gamma, s->st);
     }
 };
 

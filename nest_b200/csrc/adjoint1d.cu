@@ -9,4 +9,9 @@ cudaError_t launch_1d_adjoint_stage(const double* U, const double* Lout, const d
     return launch_1d_adjoint_stage_t<double>(U, Lout, Extra, Lin, n, h, dtp, dx, gamma, alpha, beta, st);
 }
 
+cudaError_t launch_1d_adjoint_step(const double* Un, const double* U1, const double* lam, double* lam_new, int n,
+                                   int h, const double* dtp, double dx, double gamma, cudaStream_t st) {
+    return launch_1d_adjoint_step_t<double>(Un, U1, lam, lam_new, n, h, dtp, dx, gamma, st);
+}
+
 }  // namespace nestb

@@ -27,7 +27,8 @@
 namespace nestb {
 namespace {
 
-constexpr int TA = 128;  // cells per CTA
+constexpr int TA = 128;       // cells per CTA
+constexpr int NTA = TA + 10;  // threads per CTA: one per cell of the widest phase (TA + 4 outputs + 6)
 
 template <typename T>
 struct St3 { T r, u, p; };
@@ -105,92 +106,159 @@ __device__ __forceinline__ int wrap(int c, int n) {
     return r < 0 ? r + n : r;
 }
 
-// Lin = alpha * adj(U, Lout) + beta * Extra (Extra may be null).  U, Lout,
-// Extra, Lin: SoA [3][n + 2h], interior at offset h; periodic.
-template <typename T>
-__global__ void __launch_bounds__(TA)
-k1d_adjoint_stage(const T* __restrict__ U, const T* __restrict__ Lout, const T* __restrict__ Extra,
-                  T* __restrict__ Lin, int n, int h, const double* dtp, double dx, double gamma_d, double alpha_d,
-                  double beta_d) {
-    const T lambda = (T)(*dtp / dx);
-    const T gamma = (T)gamma_d, alpha = (T)alpha_d, beta = (T)beta_d;
-    __shared__ T W[3][TA + 6];     // cells c0-3 .. c0+TA+2
-    __shared__ T Lo[3][TA + 4];    // cells c0-2 .. c0+TA+1 (alpha applied)
-    __shared__ T S[3][TA + 4];     // slopes of cells c0-2 .. c0+TA+1
-    __shared__ signed char B[3][TA + 4];  // minmod branch: 0 none, 1 d1, 2 d2
-    __shared__ T WL[3][TA + 3], WR[3][TA + 3];  // face state adjoints, faces c0-2+1/2 .. c0+TA+1/2
-    __shared__ T Sb[3][TA + 2];    // slope adjoints, cells c0-1 .. c0+TA
+// Shared-memory work arrays of one reverse stage over up to NOC output cells.
+template <typename T, int NOC>
+struct Rev1 {
+    T W[3][NOC + 6];               // primitives of cells c0-3 ..
+    T Lo[3][NOC + 4];              // output adjoint of cells c0-2 .. (alpha applied)
+    T S[3][NOC + 4];               // slopes of cells c0-2 ..
+    signed char B[3][NOC + 4];     // minmod branch: 0 none, 1 d1, 2 d2
+    T WL[3][NOC + 3], WR[3][NOC + 3];  // face state adjoints, faces c0-2+1/2 ..
+    T Sb[3][NOC + 2];              // slope adjoints, cells c0-1 ..
+};
+
+// One reverse stage over the NO output cells c0 .. c0+NO-1 (wrapped
+// periodically), run by the CTA's NTA threads: Lo[t] = alpha * lo(k, t) for
+// cell c0-2+t, W from U; calls put(q, rb, mb, Eb) with q < NO and the
+// stage's Jacobian-transpose term of cell c0+q (the caller adds Lo[q + 2]
+// and any Extra).  Ends with the CTA synchronised.
+template <typename T, int NO, int NOC, class LoFn, class PutFn>
+__device__ __forceinline__ void rev_stage(Rev1<T, NOC>& R, const T* __restrict__ U, int n, int h, int c0, T lambda,
+                                          T gamma, T gm1, T alpha, LoFn lo, PutFn put) {
+    static_assert(NO <= NOC, "work arrays too small");
     const int nt = n + 2 * h;
-    const int c0 = blockIdx.x * TA;
-    const T gm1 = (T)(gamma_d - 1.0);
-    for (int t = threadIdx.x; t < TA + 6; t += TA) {
+    for (int t = threadIdx.x; t < NO + 6; t += NTA) {
         int c = wrap(c0 - 3 + t, n) + h;
         T rho = U[c], mom = U[nt + c], erg = U[2 * nt + c];
-        W[0][t] = rho; W[1][t] = mom / rho; W[2][t] = eos_pressure(gm1, rho, mom, erg);
+        R.W[0][t] = rho; R.W[1][t] = mom / rho; R.W[2][t] = eos_pressure(gm1, rho, mom, erg);
     }
-    for (int t = threadIdx.x; t < TA + 4; t += TA) {
-        int c = wrap(c0 - 2 + t, n) + h;
-        for (int k = 0; k < 3; ++k) Lo[k][t] = alpha * Lout[k * nt + c];
-    }
+    for (int t = threadIdx.x; t < NO + 4; t += NTA)
+        for (int k = 0; k < 3; ++k) R.Lo[k][t] = alpha * lo(k, t);
     __syncthreads();
-    for (int t = threadIdx.x; t < TA + 4; t += TA) {  // cell c0-2+t <-> W index t+1
+    for (int t = threadIdx.x; t < NO + 4; t += NTA) {  // cell c0-2+t <-> W index t+1
         for (int k = 0; k < 3; ++k) {
-            T d1 = W[k][t + 1] - W[k][t], d2 = W[k][t + 2] - W[k][t + 1];
+            T d1 = R.W[k][t + 1] - R.W[k][t], d2 = R.W[k][t + 2] - R.W[k][t + 1];
             T s;
             signed char br;
             if (d1 * d2 <= T(0)) { s = T(0); br = 0; }
             else if (fabs(d1) < fabs(d2)) { s = d1; br = 1; }
             else { s = d2; br = 2; }
-            S[k][t] = s; B[k][t] = br;
+            R.S[k][t] = s; R.B[k][t] = br;
         }
     }
     __syncthreads();
-    // faces: f = 0 .. TA+2 between cells a = c0-2+f and b = a+1 (S/Lo index f and f+1)
-    for (int f = threadIdx.x; f < TA + 3; f += TA) {
-        St3<T> L = { W[0][f + 1] + T(0.5) * S[0][f], W[1][f + 1] + T(0.5) * S[1][f], W[2][f + 1] + T(0.5) * S[2][f] };
-        St3<T> R = { W[0][f + 2] - T(0.5) * S[0][f + 1], W[1][f + 2] - T(0.5) * S[1][f + 1], W[2][f + 2] - T(0.5) * S[2][f + 1] };
+    // faces: f = 0 .. NO+2 between cells a = c0-2+f and b = a+1 (S/Lo index f and f+1)
+    for (int f = threadIdx.x; f < NO + 3; f += NTA) {
+        St3<T> L = { R.W[0][f + 1] + T(0.5) * R.S[0][f], R.W[1][f + 1] + T(0.5) * R.S[1][f],
+                     R.W[2][f + 1] + T(0.5) * R.S[2][f] };
+        St3<T> Rs = { R.W[0][f + 2] - T(0.5) * R.S[0][f + 1], R.W[1][f + 2] - T(0.5) * R.S[1][f + 1],
+                      R.W[2][f + 2] - T(0.5) * R.S[2][f + 1] };
         T fb[3], wl[3] = {0, 0, 0}, wr[3] = {0, 0, 0};
-        for (int k = 0; k < 3; ++k) fb[k] = lambda * (Lo[k][f + 1] - Lo[k][f]);
-        hlle1d_adj(gamma, gm1, L, R, fb, wl, wr);
-        for (int k = 0; k < 3; ++k) { WL[k][f] = wl[k]; WR[k][f] = wr[k]; }
+        for (int k = 0; k < 3; ++k) fb[k] = lambda * (R.Lo[k][f + 1] - R.Lo[k][f]);
+        hlle1d_adj(gamma, gm1, L, Rs, fb, wl, wr);
+        for (int k = 0; k < 3; ++k) { R.WL[k][f] = wl[k]; R.WR[k][f] = wr[k]; }
     }
     __syncthreads();
-    // slope adjoints of cells c0-1 .. c0+TA (index q): right face q+1, left face q
-    for (int q = threadIdx.x; q < TA + 2; q += TA)
-        for (int k = 0; k < 3; ++k) Sb[k][q] = T(0.5) * WL[k][q + 1] - T(0.5) * WR[k][q];
+    // slope adjoints of cells c0-1 .. c0+NO (index q): right face q+1, left face q
+    for (int q = threadIdx.x; q < NO + 2; q += NTA)
+        for (int k = 0; k < 3; ++k) R.Sb[k][q] = T(0.5) * R.WL[k][q + 1] - T(0.5) * R.WR[k][q];
     __syncthreads();
-    int i = c0 + threadIdx.x;
-    if (i >= n) return;
-    const int q = threadIdx.x + 1;  // Sb index of cell i; S/B index q+1; faces q (left), q+1 (right)
-    T wb[3];
-    for (int k = 0; k < 3; ++k) {
-        T v = WR[k][q] + WL[k][q + 1];
-        int b0 = B[k][q + 1], bm = B[k][q], bp = B[k][q + 2];
-        if (b0 == 1) v += Sb[k][q];
-        else if (b0 == 2) v -= Sb[k][q];
-        if (bm == 2) v += Sb[k][q - 1];
-        if (bp == 1) v -= Sb[k][q + 1];
-        wb[k] = v;
+    for (int c = threadIdx.x; c < NO; c += NTA) {
+        const int q = c + 1;  // Sb index of cell c0+c; S/B index q+1; faces q (left), q+1 (right)
+        T wb[3];
+        for (int k = 0; k < 3; ++k) {
+            T v = R.WR[k][q] + R.WL[k][q + 1];
+            int b0 = R.B[k][q + 1], bm = R.B[k][q], bp = R.B[k][q + 2];
+            if (b0 == 1) v += R.Sb[k][q];
+            else if (b0 == 2) v -= R.Sb[k][q];
+            if (bm == 2) v += R.Sb[k][q - 1];
+            if (bp == 1) v -= R.Sb[k][q + 1];
+            wb[k] = v;
+        }
+        // (rho, u, p) = prim(rho, m, E): transpose of its Jacobian at the cell
+        const int e = wrap(c0 + c, n) + h;
+        T rho = U[e], mom = U[nt + e], erg = U[2 * nt + e];
+        T u = mom / rho, ir = T(1) / rho;
+        T praw = gm1 * (erg - T(0.5) * rho * u * u);
+        T act = (praw < T(0)) ? T(0) : T(1);
+        T rb = wb[0] - wb[1] * u * ir + act * wb[2] * gm1 * T(0.5) * u * u;
+        T mb = wb[1] * ir - act * wb[2] * gm1 * u;
+        T Eb = act * wb[2] * gm1;
+        put(c, rb, mb, Eb);
     }
-    // (rho, u, p) = prim(rho, m, E): transpose of its Jacobian at cell i
-    int e = h + i;
-    T rho = U[e], mom = U[nt + e], erg = U[2 * nt + e];
-    T u = mom / rho, ir = T(1) / rho;
-    T praw = gm1 * (erg - T(0.5) * rho * u * u);
-    T act = (praw < T(0)) ? T(0) : T(1);
-    T rb = wb[0] - wb[1] * u * ir + act * wb[2] * gm1 * T(0.5) * u * u;
-    T mb = wb[1] * ir - act * wb[2] * gm1 * u;
-    T Eb = act * wb[2] * gm1;
-    T out[3] = { Lo[0][q + 1] + rb, Lo[1][q + 1] + mb, Lo[2][q + 1] + Eb };
+    __syncthreads();
+}
+
+// Output of a reverse stage into the solver layout, with the adjoint's ghost
+// cells kept consistent with the periodic wrap.
+template <typename T>
+__device__ __forceinline__ void put_global(T* Lin, int n, int h, int i, const T v[3]) {
+    const int nt = n + 2 * h, e = h + i;
     for (int k = 0; k < 3; ++k) {
-        T v = out[k];
-        if (Extra) v += beta * Extra[k * nt + e];
-        Lin[k * nt + e] = v;
+        Lin[k * nt + e] = v[k];
+        if (i < h) Lin[k * nt + h + n + i] = v[k];
+        if (i >= n - h) Lin[k * nt + (i - (n - h))] = v[k];
     }
-    // keep the adjoint's ghost cells consistent with the periodic wrap
-    for (int k = 0; k < 3; ++k) {
-        if (i < h) Lin[k * nt + h + n + i] = Lin[k * nt + e];
-        if (i >= n - h) Lin[k * nt + (i - (n - h))] = Lin[k * nt + e];
+}
+
+// Lin = alpha * adj(U, Lout) + beta * Extra (Extra may be null).  U, Lout,
+// Extra, Lin: SoA [3][n + 2h], interior at offset h; periodic.
+template <typename T>
+__global__ void __launch_bounds__(NTA)
+k1d_adjoint_stage(const T* __restrict__ U, const T* __restrict__ Lout, const T* __restrict__ Extra,
+                  T* __restrict__ Lin, int n, int h, const double* dtp, double dx, double gamma_d, double alpha_d,
+                  double beta_d) {
+    __shared__ Rev1<T, TA> R;
+    const T lambda = (T)(*dtp / dx);
+    const T gamma = (T)gamma_d, alpha = (T)alpha_d, beta = (T)beta_d, gm1 = (T)(gamma_d - 1.0);
+    const int nt = n + 2 * h, c0 = blockIdx.x * TA;
+    auto lo = [&](int k, int t) { return Lout[k * nt + wrap(c0 - 2 + t, n) + h]; };
+    auto put = [&](int c, T rb, T mb, T Eb) {
+        const int i = c0 + c;
+        if (i >= n) return;
+        const int e = h + i;
+        T v[3] = { R.Lo[0][c + 2] + rb, R.Lo[1][c + 2] + mb, R.Lo[2][c + 2] + Eb };
+        if (Extra)
+            for (int k = 0; k < 3; ++k) v[k] += beta * Extra[k * nt + e];
+        put_global(Lin, n, h, i, v);
+    };
+    rev_stage<T, TA>(R, U, n, h, c0, lambda, gamma, gm1, alpha, lo, put);
+}
+
+// One reverse Heun step in one launch: tmp = S'(U1)^T lam / 2 over the CTA's
+// cells and a two-cell halo on each side (kept in shared memory), then
+// lam_new = S'(Un)^T tmp + lam / 2 over its cells.  Same arithmetic as two
+// k1d_adjoint_stage launches (the halo's tmp is recomputed by both
+// neighbouring CTAs, bit for bit the same).
+template <typename T>
+__global__ void __launch_bounds__(NTA)
+k1d_adjoint_step(const T* __restrict__ Un, const T* __restrict__ U1, const T* __restrict__ lam,
+                 T* __restrict__ lam_new, int n, int h, const double* dtp, double dx, double gamma_d) {
+    __shared__ Rev1<T, TA + 4> R;
+    __shared__ T tmp[3][TA + 4];  // cells c0-2 .. c0+TA+1
+    const T lambda = (T)(*dtp / dx);
+    const T gamma = (T)gamma_d, gm1 = (T)(gamma_d - 1.0);
+    const int nt = n + 2 * h, c0 = blockIdx.x * TA;
+    {
+        auto lo = [&](int k, int t) { return lam[k * nt + wrap(c0 - 4 + t, n) + h]; };
+        auto put = [&](int c, T rb, T mb, T Eb) {
+            tmp[0][c] = R.Lo[0][c + 2] + rb;
+            tmp[1][c] = R.Lo[1][c + 2] + mb;
+            tmp[2][c] = R.Lo[2][c + 2] + Eb;
+        };
+        rev_stage<T, TA + 4>(R, U1, n, h, c0 - 2, lambda, gamma, gm1, T(0.5), lo, put);
+    }
+    {
+        auto lo = [&](int k, int t) { return tmp[k][t]; };
+        auto put = [&](int c, T rb, T mb, T Eb) {
+            const int i = c0 + c;
+            if (i >= n) return;
+            const int e = h + i;
+            T v[3] = { R.Lo[0][c + 2] + rb, R.Lo[1][c + 2] + mb, R.Lo[2][c + 2] + Eb };
+            for (int k = 0; k < 3; ++k) v[k] += T(0.5) * lam[k * nt + e];
+            put_global(lam_new, n, h, i, v);
+        };
+        rev_stage<T, TA>(R, Un, n, h, c0, lambda, gamma, gm1, T(1), lo, put);
     }
 }
 
@@ -198,7 +266,15 @@ template <typename T>
 cudaError_t launch_1d_adjoint_stage_t(const T* U, const T* Lout, const T* Extra, T* Lin, int n, int h, const double* dtp,
                                       double dx, double gamma, double alpha, double beta, cudaStream_t st) {
     int blocks = (n + TA - 1) / TA;
-    k1d_adjoint_stage<T><<<blocks, TA, 0, st>>>(U, Lout, Extra, Lin, n, h, dtp, dx, gamma, alpha, beta);
+    k1d_adjoint_stage<T><<<blocks, NTA, 0, st>>>(U, Lout, Extra, Lin, n, h, dtp, dx, gamma, alpha, beta);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_1d_adjoint_step_t(const T* Un, const T* U1, const T* lam, T* lam_new, int n, int h,
+                                     const double* dtp, double dx, double gamma, cudaStream_t st) {
+    int blocks = (n + TA - 1) / TA;
+    k1d_adjoint_step<T><<<blocks, NTA, 0, st>>>(Un, U1, lam, lam_new, n, h, dtp, dx, gamma);
     return cudaGetLastError();
 }
 

@@ -10,4 +10,9 @@ cudaError_t launch_1d_adjoint_stage_f32(const float* U, const float* Lout, const
     return launch_1d_adjoint_stage_t<float>(U, Lout, Extra, Lin, n, h, dtp, dx, gamma, alpha, beta, st);
 }
 
+cudaError_t launch_1d_adjoint_step_f32(const float* Un, const float* U1, const float* lam, float* lam_new, int n,
+                                       int h, const double* dtp, double dx, double gamma, cudaStream_t st) {
+    return launch_1d_adjoint_step_t<float>(Un, U1, lam, lam_new, n, h, dtp, dx, gamma, st);
+}
+
 }  // namespace nestb
