@@ -4,7 +4,7 @@
 // form, fast reciprocal / square root).  Time, dt and the wave-speed maximum
 // stay FP64 in both.
 //
-// One CTA of T1 threads owns T1 cells: primitives of its cells and a 2-cell
+// One CTA of T1 + 32 threads owns T1 cells: primitives of its cells and a 2-cell
 // halo into shared memory, one HLLE per face, the update with the ghost
 // copies it feeds; stage 2 fuses the Heun average and the block's max
 // |u|+c (one atomic per block).  dt is derived on the device from that
@@ -18,7 +18,11 @@
 namespace nestb {
 namespace {
 
-constexpr int T1 = 256;  // cells per tile = threads per block
+constexpr int T1 = 256;       // cells per tile
+// threads per block: at least one per extended cell (T1 + 4), so that no
+// phase loops twice, in whole warps (the stage-2 reduction shuffles over
+// full warps)
+constexpr int NT1 = T1 + 32;
 
 // Max |u|+c of one cell (benchmark_euler1d.cpp:170-178).
 template <typename T>
@@ -42,7 +46,7 @@ __device__ __forceinline__ void push_ghosts_1d(T* U, int nt, int k, int c, int n
 }
 
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(T1)
+__global__ void __launch_bounds__(NT1)
 k1d_stage(const T* __restrict__ Uin, const T* Un, T* Uout,
           int n, int h, double dx, double gamma_d, int bc, LoopParams lp, StepCtrl* ctrl, int p) {
     __shared__ T W[3][T1 + 4];
@@ -70,7 +74,7 @@ k1d_stage(const T* __restrict__ Uin, const T* Un, T* Uout,
     const T dtdx = (T)(dt / dx);
     int c0 = blockIdx.x * T1;  // first interior cell of the tile
     // primitives of extended cells c0-2 .. c0+T1+1 (clamped at the array end)
-    for (int t = threadIdx.x; t < T1 + 4; t += T1) {
+    for (int t = threadIdx.x; t < T1 + 4; t += NT1) {
         int e = min(h + c0 - 2 + t, nt - 1);
         T rho = Uin[e], mom = Uin[nt + e], erg = Uin[2 * nt + e];
         W[0][t] = rho;
@@ -79,7 +83,7 @@ k1d_stage(const T* __restrict__ Uin, const T* Un, T* Uout,
     }
     __syncthreads();
     int nf = min(T1, n - c0) + 1;  // faces of this tile
-    for (int f = threadIdx.x; f < nf; f += T1) {
+    for (int f = threadIdx.x; f < nf; f += NT1) {
         int a = f + 1, b = f + 2;  // tile-local W indices around the face
         T sa[3], sb[3];
 #pragma unroll
@@ -95,7 +99,7 @@ k1d_stage(const T* __restrict__ Uin, const T* Un, T* Uout,
     __syncthreads();
     int c = c0 + threadIdx.x;
     double ms = 0.0;
-    if (c < n) {
+    if (threadIdx.x < T1 && c < n) {
         int e = h + c;
         T v[3];
 #pragma unroll
@@ -116,7 +120,7 @@ k1d_stage(const T* __restrict__ Uin, const T* Un, T* Uout,
         if (l == 0) red[w] = ms;
         __syncthreads();
         if (w == 0) {
-            double x = (l < T1 / 32) ? red[l] : 0.0;
+            double x = (l < (NT1 + 31) / 32) ? red[l] : 0.0;
             x = warp_max(x);
             if (l == 0) {
                 if (!(x == x) || x > 1.79e308) atomicOr(&ctrl->err, ERRW_NONFINITE);
@@ -167,8 +171,8 @@ template <typename T>
 cudaError_t launch_1d_step_t(T* U, T* U1, int n, int h, double dx, double gamma, int bc, const LoopParams& lp,
                              StepCtrl* ctrl, int p, int which, cudaStream_t st, T* Uout) {
     int blocks = (n + T1 - 1) / T1;
-    if (which & 1) k1d_stage<T, 1><<<blocks, T1, 0, st>>>(U, nullptr, U1, n, h, dx, gamma, bc, lp, ctrl, p);
-    if (which & 2) k1d_stage<T, 2><<<blocks, T1, 0, st>>>(U1, U, Uout ? Uout : U, n, h, dx, gamma, bc, lp, ctrl, p);
+    if (which & 1) k1d_stage<T, 1><<<blocks, NT1, 0, st>>>(U, nullptr, U1, n, h, dx, gamma, bc, lp, ctrl, p);
+    if (which & 2) k1d_stage<T, 2><<<blocks, NT1, 0, st>>>(U1, U, Uout ? Uout : U, n, h, dx, gamma, bc, lp, ctrl, p);
     return cudaGetLastError();
 }
 
