@@ -30,12 +30,6 @@ using namespace nestb;
 using namespace nestb::rt;
 
 namespace nestb {
-cudaError_t launch_1d_adjoint_stage(const double* U, const double* Lout, const double* Extra, double* Lin, int n,
-                                    int h, const double* dtp, double dx, double gamma, double alpha, double beta,
-                                    cudaStream_t st);
-cudaError_t launch_1d_adjoint_stage_f32(const float* U, const float* Lout, const float* Extra, float* Lin, int n,
-                                        int h, const double* dtp, double dx, double gamma, double alpha, double beta,
-                                        cudaStream_t st);
 // Both reverse stages of one Heun step in one launch (the intermediate adjoint
 // stays in shared memory).
 cudaError_t launch_1d_adjoint_step(const double* Un, const double* U1, const double* lam, double* lam_new, int n,

@@ -1,13 +1,7 @@
-// FP64 instantiation of the 1D adjoint stage (adjoint1d.cuh).
+// FP64 instantiation of the 1D reverse step (adjoint1d.cuh).
 #include "adjoint1d.cuh"
 
 namespace nestb {
-
-cudaError_t launch_1d_adjoint_stage(const double* U, const double* Lout, const double* Extra, double* Lin, int n,
-                                    int h, const double* dtp, double dx, double gamma, double alpha, double beta,
-                                    cudaStream_t st) {
-    return launch_1d_adjoint_stage_t<double>(U, Lout, Extra, Lin, n, h, dtp, dx, gamma, alpha, beta, st);
-}
 
 cudaError_t launch_1d_adjoint_step(const double* Un, const double* U1, const double* lam, double* lam_new, int n,
                                    int h, const double* dtp, double dx, double gamma, cudaStream_t st) {

@@ -201,35 +201,10 @@ __device__ __forceinline__ void put_global(T* Lin, int n, int h, int i, const T 
     }
 }
 
-// Lin = alpha * adj(U, Lout) + beta * Extra (Extra may be null).  U, Lout,
-// Extra, Lin: SoA [3][n + 2h], interior at offset h; periodic.
-template <typename T>
-__global__ void __launch_bounds__(NTA)
-k1d_adjoint_stage(const T* __restrict__ U, const T* __restrict__ Lout, const T* __restrict__ Extra,
-                  T* __restrict__ Lin, int n, int h, const double* dtp, double dx, double gamma_d, double alpha_d,
-                  double beta_d) {
-    __shared__ Rev1<T, TA> R;
-    const T lambda = (T)(*dtp / dx);
-    const T gamma = (T)gamma_d, alpha = (T)alpha_d, beta = (T)beta_d, gm1 = (T)(gamma_d - 1.0);
-    const int nt = n + 2 * h, c0 = blockIdx.x * TA;
-    auto lo = [&](int k, int t) { return Lout[k * nt + wrap(c0 - 2 + t, n) + h]; };
-    auto put = [&](int c, T rb, T mb, T Eb) {
-        const int i = c0 + c;
-        if (i >= n) return;
-        const int e = h + i;
-        T v[3] = { R.Lo[0][c + 2] + rb, R.Lo[1][c + 2] + mb, R.Lo[2][c + 2] + Eb };
-        if (Extra)
-            for (int k = 0; k < 3; ++k) v[k] += beta * Extra[k * nt + e];
-        put_global(Lin, n, h, i, v);
-    };
-    rev_stage<T, TA>(R, U, n, h, c0, lambda, gamma, gm1, alpha, lo, put);
-}
-
 // One reverse Heun step in one launch: tmp = S'(U1)^T lam / 2 over the CTA's
 // cells and a two-cell halo on each side (kept in shared memory), then
-// lam_new = S'(Un)^T tmp + lam / 2 over its cells.  Same arithmetic as two
-// k1d_adjoint_stage launches (the halo's tmp is recomputed by both
-// neighbouring CTAs, bit for bit the same).
+// lam_new = S'(Un)^T tmp + lam / 2 over its cells (the halo's tmp is
+// recomputed by both neighbouring CTAs, bit for bit the same).
 template <typename T>
 __global__ void __launch_bounds__(NTA)
 k1d_adjoint_step(const T* __restrict__ Un, const T* __restrict__ U1, const T* __restrict__ lam,
@@ -260,14 +235,6 @@ k1d_adjoint_step(const T* __restrict__ Un, const T* __restrict__ U1, const T* __
         };
         rev_stage<T, TA>(R, Un, n, h, c0, lambda, gamma, gm1, T(1), lo, put);
     }
-}
-
-template <typename T>
-cudaError_t launch_1d_adjoint_stage_t(const T* U, const T* Lout, const T* Extra, T* Lin, int n, int h, const double* dtp,
-                                      double dx, double gamma, double alpha, double beta, cudaStream_t st) {
-    int blocks = (n + TA - 1) / TA;
-    k1d_adjoint_stage<T><<<blocks, NTA, 0, st>>>(U, Lout, Extra, Lin, n, h, dtp, dx, gamma, alpha, beta);
-    return cudaGetLastError();
 }
 
 template <typename T>
