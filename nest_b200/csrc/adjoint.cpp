@@ -173,13 +173,20 @@ nest_status copy_state_dev(nest_adjoint* a, void* dst, const void* src) {
     return NEST_OK;
 }
 
-// Advance `work` (holding the state at step j0) by k steps.
-nest_status advance_work(nest_adjoint* a, int j0, int k) {
-    for (int j = j0; j < j0 + k; ++j) {
-        cudaError_t e = a->stepper->stage(1, a->work, a->u1, nullptr, fixed(a->dts[j]), 0);
-        if (e == cudaSuccess) e = a->stepper->stage(2, a->work, a->u1, nullptr, fixed(a->dts[j]), 0);
+// Advance the state of step j0 held in `src` by k >= 1 steps into `dst`
+// without copying it first: the first step reads `src` (left unchanged), the
+// steps between run in place in `work`, the last step writes `dst` (which may
+// be `work`) out of place.
+nest_status advance_from(nest_adjoint* a, void* src, void* dst, int j0, int k) {
+    void* in = src;
+    for (int s = 0; s < k; ++s) {
+        const int j = j0 + s;
+        void* out = (s == k - 1) ? dst : a->work;
+        cudaError_t e = a->stepper->stage(1, in, a->u1, nullptr, fixed(a->dts[j]), 0);
+        if (e == cudaSuccess) e = a->stepper->stage(2, in, a->u1, out == in ? nullptr : out, fixed(a->dts[j]), 0);
         if (e != cudaSuccess) return cuda_fail(e, "recompute step");
         ++a->advanced;
+        in = out;
     }
     return NEST_OK;
 }
@@ -200,12 +207,11 @@ nest_status reverse_binomial(nest_adjoint* a, int l, int r, int k, int free, int
     int t = r - l;
     if (t == 1) return reverse_one(a, a->slots[k], l, cur);
     if (free == 0) {
-        for (int j = r - 1; j >= l; --j) {
-            if ((st = copy_state_dev(a, a->work, a->slots[k])) != NEST_OK) return st;
-            if ((st = advance_work(a, l, j - l)) != NEST_OK) return st;
+        for (int j = r - 1; j > l; --j) {
+            if ((st = advance_from(a, a->slots[k], a->work, l, j - l)) != NEST_OK) return st;
             if ((st = reverse_one(a, a->work, j, cur)) != NEST_OK) return st;
         }
-        return NEST_OK;
+        return reverse_one(a, a->slots[k], l, cur);
     }
     int rep = 1;
     while (binom(free + rep, free) < t) ++rep;
@@ -213,9 +219,7 @@ nest_status reverse_binomial(nest_adjoint* a, int l, int r, int k, int free, int
     d = std::max<long long>(1, std::min<long long>(d, t - 1));
     int m = l + (int)d;
     if (a->slot_pos[k + 1] != m) {
-        if ((st = copy_state_dev(a, a->work, a->slots[k])) != NEST_OK) return st;
-        if ((st = advance_work(a, l, m - l)) != NEST_OK) return st;
-        if ((st = copy_state_dev(a, a->slots[k + 1], a->work)) != NEST_OK) return st;
+        if ((st = advance_from(a, a->slots[k], a->slots[k + 1], l, m - l)) != NEST_OK) return st;
         a->slot_pos[k + 1] = m;
     }
     if ((st = reverse_binomial(a, m, r, k + 1, free - 1, cur)) != NEST_OK) return st;
