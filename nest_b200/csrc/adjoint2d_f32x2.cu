@@ -140,25 +140,21 @@ __device__ __forceinline__ void hlle2_adj(float gamma, float igm1, const Q4& L, 
     F2 D = sub2(mul2(pL, YL), mul2(pR, YR));
     F2 s1 = add2(fma2(sub2(nL, sr), ZL, D), mul2(sub2(sr, nR), ZR));
     F2 s2 = sub2(fma2(add2(nR, nsl), ZR, mul2(sp(-1.f), D)), mul2(add2(nL, nsl), ZL));
-    F2 i2 = mul2(inv, inv);
+    // the speed adjoints apply only where both clamps are open (subsonic):
+    // in the supersonic regimes one of nsl, sr is 0 and the other adjoint is
+    // 0 by its own factor, so one mask serves both
+    F2 i2 = mul2(mul2(inv, inv), make_float2(nsl.x * sr.x > 0.f ? 1.f : 0.f, nsl.y * sr.y > 0.f ? 1.f : 0.f));
     F2 Slb = mul2(mul2(sr, i2), s1);               // adjoint of S_L
     F2 Srb = mul2(mul2(sp(-1.f), mul2(nsl, i2)), s2);  // adjoint of S_R
-    // clamps and active arguments (S_L = min(nL - cL, nR - cR), S_R = max(nL + cL, nR + cR);
-    // the right argument is active only where strictly smaller / larger)
-    F2 nbL, cbL, nbR, cbR;
-    {
-        float sLx = nsl.x > 0.f ? Slb.x : 0.f, sLy = nsl.y > 0.f ? Slb.y : 0.f;
-        float sRx = sr.x > 0.f ? Srb.x : 0.f, sRy = sr.y > 0.f ? Srb.y : 0.f;
-        // nR - cR < nL - cL  <=>  cR - nR > cL - nL (exact negations)
-        const bool lrx = aR.x > aL.x, lry = aR.y > aL.y;
-        const bool rrx = bL.x < bR.x, rry = bL.y < bR.y;
-        F2 sl_L = make_float2(lrx ? 0.f : sLx, lry ? 0.f : sLy);
-        F2 sl_R = make_float2(lrx ? sLx : 0.f, lry ? sLy : 0.f);
-        F2 sr_L = make_float2(rrx ? 0.f : sRx, rry ? 0.f : sRy);
-        F2 sr_R = make_float2(rrx ? sRx : 0.f, rry ? sRy : 0.f);
-        nbL = add2(sl_L, sr_L); cbL = sub2(sr_L, sl_L);
-        nbR = add2(sl_R, sr_R); cbR = sub2(sr_R, sl_R);
-    }
+    // active arguments (S_L = min(nL - cL, nR - cR), S_R = max(nL + cL, nR + cR);
+    // the right argument only where strictly smaller / larger; nR - cR < nL - cL
+    // <=> cR - nR > cL - nL, exact negations)
+    F2 mL = make_float2(aR.x > aL.x ? 1.f : 0.f, aR.y > aL.y ? 1.f : 0.f);
+    F2 mR = make_float2(bL.x < bR.x ? 1.f : 0.f, bL.y < bR.y ? 1.f : 0.f);
+    F2 sl_R = mul2(mL, Slb), sl_L = sub2(Slb, sl_R);
+    F2 sr_R = mul2(mR, Srb), sr_L = sub2(Srb, sr_R);
+    F2 nbL = add2(sl_L, sr_L), cbL = sub2(sr_L, sl_L);
+    F2 nbR = add2(sl_R, sr_R), cbR = sub2(sr_R, sl_R);
     // sound-speed derivatives, zero where p = 0 (c = 0)
     F2 hL = make_float2(pL.x > 0.f ? 0.5f * qL.x : 0.f, pL.y > 0.f ? 0.5f * qL.y : 0.f);
     F2 hR = make_float2(pR.x > 0.f ? 0.5f * qR.x : 0.f, pR.y > 0.f ? 0.5f * qR.y : 0.f);
@@ -213,18 +209,22 @@ __global__ void __maxnreg__(NEST_ADJX2_REGS) k2d_adjoint_x2(AdjX2Args A) {
     const long long coff = cw + 2;
     const bool out_a = lane >= 2 && lane <= 29 && ca < ny;
     const bool out_b = lane >= 2 && lane <= 29 && ca + 1 < ny;
-    auto rowoff = [&](int i) {
+    auto wrapr = [&](int i) {
         int r = i % nx;
-        if (r < 0) r += nx;
-        return (long long)(r + 2) * pitch + coff;
+        return r < 0 ? r + nx : r;
     };
+    auto rowoff = [&](int i) { return (long long)(wrapr(i) + 2) * pitch + coff; };
+    // wrapped rows of the three streams issued at march step a (conserved
+    // row a+3, Lout row a+2, Extra row a), advanced by one per step
+    auto next_row = [&](int& r) { r = (r + 1 == nx) ? 0 : r + 1; };
+    int ru = wrapr(r0 + 1), rl = wrapr(r0), re = wrapr(r0 - 2);
 
     F2* const ring = adj_ring + warp * RING_F2 + lane;
     F2* const ringU = ring;
     F2* const ringL = ring + RU * 128;
     F2* const ringE = ring + (RU + RL) * 128;
-    auto issue = [&](const float* base, int i, F2* slot) {
-        const float* q = base + rowoff(i);
+    auto issue_row = [&](const float* base, int r, F2* slot) {  // r: wrapped row
+        const float* q = base + (long long)(r + 2) * pitch + coff;
         cp8(slot, q);
         cp8(slot + 32, q + vs);
         cp8(slot + 64, q + 2 * vs);
@@ -261,9 +261,9 @@ __global__ void __maxnreg__(NEST_ADJX2_REGS) k2d_adjoint_x2(AdjX2Args A) {
         s.c = mm_mask(sub2(W0.c, Wm.c), sub2(W1.c, W0.c), m1.c, m2.c);
         s.d = mm_mask(sub2(W0.d, Wm.d), sub2(W1.d, W0.d), m1.d, m2.d);
         P0 = { fma2(half, s.a, W0.a), fma2(half, s.b, W0.b), fma2(half, s.c, W0.c), fma2(half, s.d, W0.d) };
-        issue(A.U, r0, ringU + (r0 & (RU - 1)) * 128);
-        issue(A.Lout, r0 - 2, ringL + ((r0 - 2) & (RL - 1)) * 128);
-        issue(A.Lout, r0 - 1, ringL + ((r0 - 1) & (RL - 1)) * 128);
+        issue_row(A.U, wrapr(r0), ringU + (r0 & (RU - 1)) * 128);
+        issue_row(A.Lout, wrapr(r0 - 2), ringL + ((r0 - 2) & (RL - 1)) * 128);
+        issue_row(A.Lout, wrapr(r0 - 1), ringL + ((r0 - 1) & (RL - 1)) * 128);
         cp_commit();
     }
     const F2 z = sp(0.f);
@@ -272,9 +272,12 @@ __global__ void __maxnreg__(NEST_ADJX2_REGS) k2d_adjoint_x2(AdjX2Args A) {
 
 #pragma unroll AUNROLL
     for (int a = r0 - 2; a <= r0 + rows; ++a) {
-        issue(A.U, a + 3, ringU + ((a + 3) & (RU - 1)) * 128);
-        issue(A.Lout, a + 2, ringL + ((a + 2) & (RL - 1)) * 128);
-        if (has_extra) issue(A.Extra, a, ringE + (a & (RE - 1)) * 128);
+        issue_row(A.U, ru, ringU + ((a + 3) & (RU - 1)) * 128);
+        issue_row(A.Lout, rl, ringL + ((a + 2) & (RL - 1)) * 128);
+        if (has_extra) issue_row(A.Extra, re, ringE + (a & (RE - 1)) * 128);
+        next_row(ru);
+        next_row(rl);
+        next_row(re);
         cp_commit();
         cp_wait1();
 

@@ -163,18 +163,22 @@ __global__ void NEST_ADJ64_ATTR k2d_adjoint_rm64(AdjD64Args A) {
     if (cw < 0) cw += ny;
     const long long coff = cw + 2;
     const bool out = lane >= 3 && lane <= 28 && col < ny;
-    auto rowoff = [&](int i) {
+    auto wrapr = [&](int i) {
         int r = i % nx;
-        if (r < 0) r += nx;
-        return (long long)(r + 2) * pitch + coff;
+        return r < 0 ? r + nx : r;
     };
+    auto rowoff = [&](int i) { return (long long)(wrapr(i) + 2) * pitch + coff; };
+    // wrapped rows of the three streams issued at march step a (conserved
+    // row a+3, Lout row a+2, Extra row a), advanced by one per step
+    auto next_row = [&](int& r) { r = (r + 1 == nx) ? 0 : r + 1; };
+    int ru = wrapr(r0 + 1), rl = wrapr(r0), re = wrapr(r0 - 2);
 
     double* const ring = adj64_ring + warp * DRING + lane;
     double* const ringU = ring;
     double* const ringL = ring + DRU * 128;
     double* const ringE = ring + (DRU + DRL) * 128;
-    auto issue = [&](const double* base, int i, double* slot) {
-        const double* q = base + rowoff(i);
+    auto issue_row = [&](const double* base, int r, double* slot) {  // r: wrapped row
+        const double* q = base + (long long)(r + 2) * pitch + coff;
         cp8d(slot, q);
         cp8d(slot + 32, q + vs);
         cp8d(slot + 64, q + 2 * vs);
@@ -203,18 +207,21 @@ __global__ void NEST_ADJ64_ATTR k2d_adjoint_rm64(AdjD64Args A) {
               mmb(W0.c - Wm.c, W1.c - W0.c, b2), mmb(W0.d - Wm.d, W1.d - W0.d, b3) };
         brm = b0 | (b1 << 2) | (b2 << 4) | (b3 << 6);
         P0 = { W0.a + 0.5 * s.a, W0.b + 0.5 * s.b, W0.c + 0.5 * s.c, W0.d + 0.5 * s.d };
-        issue(A.U, r0, ringU + (r0 & (DRU - 1)) * 128);
-        issue(A.Lout, r0 - 2, ringL + ((r0 - 2) & (DRL - 1)) * 128);
-        issue(A.Lout, r0 - 1, ringL + ((r0 - 1) & (DRL - 1)) * 128);
+        issue_row(A.U, wrapr(r0), ringU + (r0 & (DRU - 1)) * 128);
+        issue_row(A.Lout, wrapr(r0 - 2), ringL + ((r0 - 2) & (DRL - 1)) * 128);
+        issue_row(A.Lout, wrapr(r0 - 1), ringL + ((r0 - 1) & (DRL - 1)) * 128);
         cpd_commit();
     }
     D4 Bm{ 0, 0, 0, 0 }, B0{ 0, 0, 0, 0 }, Sp{ 0, 0, 0, 0 };
 
 #pragma unroll 1
     for (int a = r0 - 2; a <= r0 + rows; ++a) {
-        issue(A.U, a + 3, ringU + ((a + 3) & (DRU - 1)) * 128);
-        issue(A.Lout, a + 2, ringL + ((a + 2) & (DRL - 1)) * 128);
-        if (has_extra) issue(A.Extra, a, ringE + (a & (DRE - 1)) * 128);
+        issue_row(A.U, ru, ringU + ((a + 3) & (DRU - 1)) * 128);
+        issue_row(A.Lout, rl, ringL + ((a + 2) & (DRL - 1)) * 128);
+        if (has_extra) issue_row(A.Extra, re, ringE + (a & (DRE - 1)) * 128);
+        next_row(ru);
+        next_row(rl);
+        next_row(re);
         cpd_commit();
         cpd_wait1();
 
