@@ -103,6 +103,30 @@ def test_uniform_and_binomial_agree(gpu):
         assert np.array_equal(o[:, 2:-2], outs[0][:, 2:-2])
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_uniform_and_binomial_agree_2d(gpu, prec):
+    """2D adjoint under the uniform schedule and under binomial schedules
+    with few and many snapshots (re-advances that start from a snapshot in
+    place and end in the next one): the same gradient bit for bit."""
+    from nest_b200.adjoint import Adjoint
+    from nest_b200.problems import kelvin_helmholtz
+    nx, ny, nsteps = 64, 48, 37
+    dt = np.float64 if prec == "f64" else np.float32
+    p = gpu.F64 if prec == "f64" else gpu.F32
+    U0 = kelvin_helmholtz(nx, ny, seed=2).astype(dt)
+    lamT = np.zeros(U0.shape, dtype=dt)
+    lamT[:, 2:-2, 2:-2] = np.random.default_rng(4).standard_normal((4, nx, ny))
+    outs = []
+    for policy, param in [(0, 10), (1, 3), (1, 9), (1, 37)]:
+        s = gpu.Solver(2, nx, ny, bc=gpu.BC_PERIODIC, precision=p)
+        s.upload(U0)
+        adj = Adjoint(s, nsteps, policy, param)
+        adj.forward(0.4)
+        outs.append(adj.backward(lamT))
+    for o in outs[1:]:
+        assert np.array_equal(o[:, 2:-2, 2:-2], outs[0][:, 2:-2, 2:-2])
+
+
 def test_autograd_rollout(gpu):
     import torch
     from nest_b200.adjoint import rollout_1d
