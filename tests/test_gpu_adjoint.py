@@ -278,6 +278,24 @@ def test_adjoint2d_fp32_row_march(gpu, nx, ny, monkeypatch):
     assert rel < 1e-4, rel
 
 
+@pytest.mark.parametrize("nx,ny", [(64, 63), (40, 27)])
+def test_adjoint2d_fp32_odd_ny(gpu, nx, ny):
+    """FP32 with an odd ny (the packed row march needs adjacent column pairs,
+    so these domains take the tile kernel) against the FP64 adjoint: smooth
+    fields, 6 steps; the two differ by FP32 rounding and the few limiter
+    branches it moves (a few 1e-4)."""
+    lam = {}
+    for prec in (gpu.F64, gpu.F32):
+        U0, s, adj = adjoint2d_case(gpu, nx, ny, 6, prec, seed=6, smooth=True)
+        UT = s.download()
+        w = np.random.default_rng(9).standard_normal((4, nx, ny))
+        lamT = np.zeros(UT.shape, dtype=UT.dtype)
+        lamT[:, 2:-2, 2:-2] = w
+        lam[prec] = adj.backward(lamT).astype(np.float64)[:, 2:-2, 2:-2]
+    rel = np.linalg.norm(lam[gpu.F32] - lam[gpu.F64]) / np.linalg.norm(lam[gpu.F64])
+    assert rel < 5e-3, rel
+
+
 @pytest.mark.parametrize("nx,ny", [(12, 10), (48, 40), (130, 118), (64, 63), (31, 77)])
 def test_adjoint2d_fp64_row_march(gpu, nx, ny, monkeypatch):
     """The FP64 row-march adjoint stage (one column per lane, strips of 26
