@@ -75,15 +75,15 @@ __device__ __forceinline__ float max3f(float a, float b, float c) {
     return t;
 }
 
-// Minmod slope of a pair and the masks of its active argument: m1 = 1 where
-// the first difference is the slope, m2 = 1 where the second is (ties: the
-// second), both 0 where the slope is 0.
-__device__ __forceinline__ F2 mm_mask(F2 d1, F2 d2, F2& m1, F2& m2) {
+// Minmod slope of a pair and the masks of its active argument: mz = 1 where
+// the slope is not 0, me = 1 where it equals the second difference (the
+// second argument is active where mz me = 1, ties included; the first where
+// mz (1 - me) = 1).  A slope adjoint sb then scatters as t2 = me (mz sb) to
+// the second difference and t1 = mz sb - t2 to the first.
+__device__ __forceinline__ F2 mm_mask(F2 d1, F2 d2, F2& mz, F2& me) {
     F2 s = make_float2(mm(d1.x, d2.x), mm(d1.y, d2.y));
-    const bool zx = s.x == 0.f, zy = s.y == 0.f;
-    const bool ex = s.x == d2.x, ey = s.y == d2.y;
-    m2 = make_float2(!zx && ex ? 1.f : 0.f, !zy && ey ? 1.f : 0.f);
-    m1 = make_float2(!zx && !ex ? 1.f : 0.f, !zy && !ey ? 1.f : 0.f);
+    mz = make_float2(s.x != 0.f ? 1.f : 0.f, s.y != 0.f ? 1.f : 0.f);
+    me = make_float2(s.x == d2.x ? 1.f : 0.f, s.y == d2.y ? 1.f : 0.f);
     return s;
 }
 
@@ -302,8 +302,8 @@ __global__ void __maxnreg__(NEST_ADJX2_REGS) k2d_adjoint_x2(AdjX2Args A) {
             // slope adjoint of row a is complete: sbar = wl/2 + Sp; scatter by the masks
             Q4 sb = { fma2(half, wl.a, Sp.a), fma2(half, wl.b, Sp.b), fma2(half, wl.c, Sp.c),
                       fma2(half, wl.d, Sp.d) };
-            auto scat = [&](F2 s, F2 k1, F2 k2, F2& bm, F2& b0, F2& b1, F2 wl_, F2 wr_) {
-                F2 t1 = mul2(k1, s), t2 = mul2(k2, s);
+            auto scat = [&](F2 s, F2 kz, F2 ke, F2& bm, F2& b0, F2& b1, F2 wl_, F2 wr_) {
+                F2 u = mul2(kz, s), t2 = mul2(ke, u), t1 = sub2(u, t2);
                 bm = sub2(bm, t1);
                 b0 = add2(b0, add2(wl_, sub2(t1, t2)));
                 b1 = add2(wr_, t2);
@@ -346,7 +346,7 @@ __global__ void __maxnreg__(NEST_ADJX2_REGS) k2d_adjoint_x2(AdjX2Args A) {
                 // first column from the left lane's second face
                 F2 q = make_float2(__shfl_up_sync(0xffffffffu, r.y, 1), r.x);
                 F2 sb = mul2(half, sub2(l, q));
-                F2 t1 = mul2(k1, sb), t2 = mul2(k2, sb);
+                F2 u = mul2(k1, sb), t2 = mul2(k2, u), t1 = sub2(u, t2);
                 F2 t1n = make_float2(t1.y, __shfl_down_sync(0xffffffffu, t1.x, 1));
                 F2 t2p = make_float2(__shfl_up_sync(0xffffffffu, t2.y, 1), t2.x);
                 b = add2(b, add2(add2(l, q), add2(sub2(t1, t2), sub2(t2p, t1n))));
