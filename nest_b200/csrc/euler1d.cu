@@ -17,6 +17,9 @@
 //     graphs by the host code).
 #include <cooperative_groups.h>
 
+#include <map>
+#include <mutex>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -441,6 +444,55 @@ static cudaError_t launch_1d_cluster(double* U, int n, int h, double dx, double 
     }
     if (clusters < 1) return cudaErrorNotSupported;
     return cudaLaunchKernelEx(&cfg, k1d_cluster, U, n, h, m, dx, gamma, bc, lp, ctrl, p);
+}
+
+// Whether launch_1d_cluster can place a cluster of 16 or 8 CTAs for n cells
+// on the current device (the chunk-size rules and the cluster occupancy query
+// of launch_1d_cluster, with nothing launched); remembered per device and n.
+bool cluster_1d_available(int n, int h) {
+    if (n < 256) return false;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, bool> known;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = known.find({dev, n});
+    if (it != known.end()) return it->second;
+    bool ok = false;
+    for (int NC : {16, 8}) {
+        const int m = (n + NC - 1) / NC;
+        if (m < 2 || n - (NC - 1) * m < 2) continue;
+        const int threads = (m + 1 + 31) / 32 * 32;
+        if (threads > 256) continue;
+        const size_t smem = sizeof(double) * (size_t)(3 * m + 3 * m + 6 * (m + 4) + 3 * (m + 1) + 32);
+        if (NC > 8 && cudaFuncSetAttribute(k1d_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        if (cudaFuncSetAttribute(k1d_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(NC, 1, 1);
+        cfg.blockDim = dim3(threads, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = NC;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, k1d_cluster, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        if (clusters >= 1) { ok = true; break; }
+    }
+    known[{dev, n}] = ok;
+    return ok;
 }
 
 cudaError_t launch_1d_resident(double* U, int n, int h, double dx, double gamma, int bc,

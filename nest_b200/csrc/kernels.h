@@ -17,6 +17,8 @@ struct Geo2D;
 
 // 1D plain form (FP64, bit-exact with nest's OpenMP path)
 size_t resident_smem_bytes(int n, int h);
+// The resident solver's cluster form can run n cells here (16 or 8 CTAs).
+bool cluster_1d_available(int n, int h);
 cudaError_t launch_1d_resident(double* U, int n, int h, double dx, double gamma, int bc,
                                const LoopParams& lp, StepCtrl* ctrl, int p, cudaStream_t st);
 cudaError_t launch_1d_prepare(double* U, int n, int h, double gamma, int bc, StepCtrl* ctrl, int p,

@@ -73,9 +73,11 @@ struct nest_solver {
     int xlo_ex = 0, xhi_ex = 0;    // sharded domain: x sides filled by a halo exchange
     std::map<nestb::rt::GraphKey, cudaGraphExec_t> graphs;
 
+    // 1D FP64 runs the resident solver when one CTA's shared memory holds the
+    // domain or a thread-block cluster can split it (up to 16 x 255 cells)
     bool resident() const {
         return d.dim == 1 && d.precision == NEST_F64 && !(d.flags & NEST_FLAG_NO_RESIDENT) &&
-               nestb::resident_smem_bytes(d.nx, h) <= 220 * 1024;
+               (nestb::resident_smem_bytes(d.nx, h) <= 220 * 1024 || nestb::cluster_1d_available(d.nx, h));
     }
     nestb::Geo2D geo() const {
         nestb::Geo2D g;

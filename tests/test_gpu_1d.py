@@ -28,10 +28,12 @@ def test_dropin_matches_reference_test(gpu):
 
 
 # 257 / 1000 cells split unevenly over the resident solver's 16-CTA cluster
-# (last chunk 2 / 55 cells)
+# (last chunk 2 / 55 cells); 3001 and 4080 cells only fit the cluster form
+# (one CTA's shared memory holds up to about 2340), 4080 = 16 x 255 its largest
 @pytest.mark.parametrize("n,bc,cfl,tf", [(1024, BC_OUTFLOW, 0.4, 0.2), (1024, BC_PERIODIC, 0.4, 0.2),
                                          (97, BC_OUTFLOW, 0.8, 0.1), (2300, BC_PERIODIC, 0.4, 0.05),
-                                         (257, BC_PERIODIC, 0.5, 0.1), (1000, BC_OUTFLOW, 0.4, 0.1)])
+                                         (257, BC_PERIODIC, 0.5, 0.1), (1000, BC_OUTFLOW, 0.4, 0.1),
+                                         (3001, BC_OUTFLOW, 0.4, 0.02), (4080, BC_PERIODIC, 0.4, 0.01)])
 @pytest.mark.parametrize("resident", [True, False])
 def test_run_to_matches_oracle(gpu, oracle, n, bc, cfl, tf, resident):
     U = sod_ic_1d(n)
