@@ -19,6 +19,9 @@
 // Each thread gathers one cell (no atomics).  Periodic indices wrap modulo n,
 // which is exactly the transpose of the periodic ghost fill
 // (benchmark_euler1d.cpp:102-110): a ghost cell's adjoint lands on its source.
+// A Heun step reverses both stages in one launch (k1d_adjoint_step): the
+// stage-2 adjoint of the CTA's cells and a two-cell halo stays in shared
+// memory and feeds the stage-1 reverse.
 #pragma once
 
 #include "common.cuh"
