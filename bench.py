@@ -5,15 +5,19 @@ Workload (default, --workload riemann2d): the 2D Euler Riemann problem on
 boundaries, CFL 0.4, gamma 1.4, 200 RK2 steps.  A bench step is one RK2 step
 of the whole grid (dt reduction, ghost fill, two fused stages).  Metric:
 cell-updates/s = interior cells x steps x 2 RK stages
-(examples/benchmark/benchmark_euler1d.cpp:217-218).  The headline form is
-FP32 (reconstruction, Riemann solve and update in FP32; FP64 dt/time); the
-FP64 plain form is measured in the same run.
+(examples/benchmark/benchmark_euler1d.cpp:217-218).  The headline form is the
+plain FP64 form, the arithmetic of the CPU path it is compared with (its
+result is checked against that CPU path cell for cell in the same run); the
+FP32 form (reconstruction, Riemann solve and update in FP32; FP64 totals,
+time, dt and positivity repair) and the plain FP32 form are measured in the
+same run under `forms`.
 
 Arms
   --impl ours       (default) the CUDA library through its C ABI.
   --impl reference  the CPU implementation of the same scheme on the host
                     cores (the oracle port: nest has no 2D RK2), one bounded
-                    sample per step.  Rank 0 only.
+                    sample per step, FP64.  Rank 0 only.  It loads neither
+                    the nest_b200 package nor its library.
 
 Multi-GPU (torchrun, N ranks): one domain of (N*4096) x 4096 cells cut into
 N x-slabs of 4096 x 4096, one per GPU (weak scaling): every step max-reduces
@@ -50,9 +54,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["riemann2d"], default="riemann2d")
     ap.add_argument("--n", type=int, default=4096, help="cells per axis")
-    ap.add_argument("--forms", default="f32,f32plain,f64",
-                    help="forms to time (f32: FP32 with FP64 totals and repair; f32plain: FP32 without them; "
-                         "f64: the plain FP64 form); the first is the headline")
+    ap.add_argument("--forms", default="f64,f32,f32plain",
+                    help="forms to time (f64: the plain FP64 form; f32: FP32 with FP64 totals and repair; "
+                         "f32plain: FP32 without them); the first is the headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
@@ -71,6 +75,34 @@ def parse():
     ap.add_argument("--extras", default="batched,adjoint1d,sod1d,adjoint2d",
                     help="comma list of extra measurements to run (with extras on)")
     return ap.parse_args()
+
+
+FORM_TEXT = {"f32": "FP32 state and arithmetic; FP64 conserved totals every step, FP64 time and dt, FP64 "
+                     "positivity repair",
+             "f32plain": "FP32 state and arithmetic; FP64 time and dt",
+             "f64": "plain FP64 form (bit for bit with the CPU oracle)"}
+
+
+def workload_config(n: int, ws: int, head: str, slab: bool) -> dict:
+    """`config` of the JSON line, the same keys for both arms."""
+    return {"workload": f"riemann2d {ws * n}x{n} {head}", "nx": ws * n, "ny": n, "form": FORM_TEXT[head],
+            "patches": f"{n // 256}x{n // 256} of 256^2" if n % 256 == 0 else "one",
+            "bc": "outflow", "cfl": 0.4, "gamma": 1.4,
+            "parallelism": "one GPU" if ws == 1 and not slab else
+            f"{ws} x-slabs of {n}x{n} (NCCL halo rows + wave-speed all-reduce)",
+            "l2": "inputs larger than L2 (two state buffers of %.0f MB each)" % (
+                4 * (n + 4) ** 2 * (4 if head.startswith("f32") else 8) / 1e6)}
+
+
+def load_problems():
+    """nest_b200/problems.py loaded by path (numpy only): the reference arm
+    builds its inputs without importing the nest_b200 package, whose import
+    loads the CUDA library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_bench_problems", ROOT / "nest_b200" / "problems.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def peaks():
@@ -347,6 +379,7 @@ def run_ours(args, ws, rank, local):
     time.sleep(0.3)
     forms = [f.strip() for f in args.forms.split(",") if f.strip()]
     launches = 0
+    final_f64 = None
     rho_final = {}
     from nest_b200.exact_riemann import l1_rho_diagonal
     for form in forms:
@@ -404,7 +437,11 @@ def run_ours(args, ws, rank, local):
         e1.record(st)
         e1.synchronize()
         graph_ms = e0.elapsed_time(e1) / args.steps
-        rho_final[form] = s.download()[0, 2:-2, 2:-2].astype(np.float64)
+        Ufin = s.download()
+        rho_final[form] = Ufin[0, 2:-2, 2:-2].astype(np.float64)
+        if form == "f64":
+            final_f64 = (Ufin, tsim, nst)
+        del Ufin
         ab = alg_bytes_per_cell(form)
         m1, m2 = float(np.mean(k1)), float(np.mean(k2))
         dom, dom_ms = ("stage2", m2) if m2 >= m1 else ("stage1", m1)
@@ -442,17 +479,7 @@ def run_ours(args, ws, rank, local):
         "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if head.startswith("f32") else "f64", "data": "synthetic",
-        "config": {"workload": f"riemann2d {ws * n}x{n} {head}", "nx": ws * n, "ny": n,
-                   "form": {"f32": "FP32 state and arithmetic; FP64 conserved totals every step, FP64 time and "
-                                   "dt, FP64 positivity repair",
-                            "f32plain": "FP32 state and arithmetic; FP64 time and dt",
-                            "f64": "plain FP64 form (bit for bit with the CPU oracle)"}[head],
-                   "patches": f"{n // 256}x{n // 256} of 256^2" if n % 256 == 0 else "one",
-                   "bc": "outflow", "cfl": cfl, "gamma": 1.4,
-                   "parallelism": "one GPU" if ws == 1 and not args.slab_path else
-                   f"{ws} x-slabs of {n}x{n} (NCCL halo rows + wave-speed all-reduce)",
-                   "l2": "inputs larger than L2 (two state buffers of %.0f MB each)" % (
-                       4 * (n + 4) ** 2 * (4 if head.startswith("f32") else 8) / 1e6)},
+        "config": workload_config(n, ws, head, args.slab_path),
         "roofline": r["roofline"],
         "forms": results,
         "e2e": r.get("e2e"),
@@ -472,7 +499,10 @@ def run_ours(args, ws, rank, local):
         out["gpu_launches_extras"] = sum(out[k]["launches"] for k in ("batched_kh", "adjoint_1d", "sod_1d")
                                          if k in out)
     if ws == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(n, args.cpu_seconds)
+        out["cpu_baseline"], parity = cpu_baseline(n, args.cpu_seconds, args.steps, final_f64)
+        if parity is not None:
+            results["f64"]["parity_vs_oracle"] = parity
+            results["f64"]["max_rel_diff_vs_oracle"] = parity["max_rel_diff"]
     return out
 
 
@@ -515,14 +545,43 @@ def bench_batch(args, ws):
     tot = b.totals()
     drift = np.abs(tot - t0).max(axis=0) / np.maximum(np.abs(t0).max(axis=0), 1e-300)
     value = cells * 2 * args.batch_steps / (ms * 1e-3)
+    # accuracy: the same problems advanced the same 2 + K steps by the plain
+    # FP64 form (one FP64 batch); L1(rho) of every problem against it
+    acc = batch_vs_f64(b, nx, ny, ids, 2 + args.batch_steps, times, st)
     b.close()
     return {"value": value, "unit": UNIT, "problems": args.batch_count, "problems_per_rank": int(len(nx)),
+            "l1_rho_vs_f64": acc,
             "sharding": f"by problem over {ws} rank(s), no collective", "cells": int(cells), "steps": args.batch_steps,
             "ms_total": ms, "ms_per_step": ms / args.batch_steps, "work_items": items, "persistent_blocks": blocks,
             "hbm_gbs_equiv_per_gpu": value / ws * 40 / 1e9, "sim_time_range": [float(times.min()), float(times.max())],
             "fp64_totals_rel_drift": {"mass": float(drift[0]), "energy": float(drift[3])},
             "tiling": {"rows_per_item": tiling[0], "warps_per_block": tiling[1], "blocks_per_sm": tiling[2]},
             "launches": 4 * args.batch_steps, "dtype": "f32 (FP64 totals, time, repair)"}
+
+
+def batch_vs_f64(b32, nx, ny, ids, nsteps, times32, st):
+    """L1(rho) of each problem of an FP32 batch against the plain FP64 form
+    run from the same initial states for the same number of steps (untimed)."""
+    import nest_b200 as nb
+    from nest_b200.problems import kelvin_helmholtz
+    b64 = nb.Batch(nx, ny, precision=nb.F64, stream=st.cuda_stream)
+    for p in range(len(nx)):
+        b64.upload(p, kelvin_helmholtz(int(nx[p]), int(ny[p]), seed=1 + int(ids[p])))
+    b64.step(nsteps, 0.4)
+    t64, _ = b64.times()
+    l1, rel = [], []
+    for p in range(len(nx)):
+        r64 = b64.download(p, nb.LAYOUT_INTERIOR)[0]
+        r32 = b32.download(p, nb.LAYOUT_INTERIOR)[0].astype(np.float64)
+        d = float(np.mean(np.abs(r32 - r64)))
+        l1.append(d)
+        rel.append(d / float(np.mean(np.abs(r64))))
+    b64.close()
+    l1, rel = np.array(l1), np.array(rel)
+    return {"steps": nsteps, "max": float(l1.max()), "median": float(np.median(l1)),
+            "max_relative_to_mean_rho": float(rel.max()),
+            "sim_time_rel_diff_max": float(np.max(np.abs(times32 - t64) / t64)),
+            "reference": "plain FP64 form, same initial states and step count"}
 
 
 def bench_adjoint(args):
@@ -733,25 +792,51 @@ def host_threads():
         return os.cpu_count() or 1
 
 
-def cpu_baseline(n: int, budget_s: float):
-    """FP64 scheme on the host cores: S RK2 steps of the full n x n problem,
-    S sized to about budget_s seconds of work."""
+def cpu_baseline(n: int, budget_s: float, steps: int, final_f64=None):
+    """FP64 scheme on the host cores (the oracle, OpenMP on every host core)
+    from the workload's initial state: after one untimed step, S steps sized
+    to about budget_s seconds are timed (the baseline); when the bench timed
+    the FP64 form, the oracle then runs on to the bench's K steps and its
+    state is compared with the GPU's final state cell for cell (the FP64
+    form's parity check at the full size, all four variables, ghost cells
+    excluded).  Returns (cpu_baseline, parity or None)."""
     from oracle.oracle import BC_OUTFLOW, Oracle
     from nest_b200.problems import riemann_2d
     orc = Oracle()
     th = host_threads()
     orc.set_threads(th)
     U = np.ascontiguousarray(riemann_2d(n, n))
+    run = lambda k: orc.run2d(U, n, n, 2, 1 / n, 1 / n, 1.4, 0.4, nsteps=k, bc=BC_OUTFLOW, record_dts=True)
+    dts = []
     t0 = time.perf_counter()
-    orc.run2d(U, n, n, 2, 1 / n, 1 / n, 1.4, 0.4, nsteps=1, bc=BC_OUTFLOW)
+    dts += list(run(1)[2])
     t1 = time.perf_counter() - t0
     S = int(max(1, min(50, budget_s / max(t1, 1e-6) - 1)))
+    if final_f64 is not None:
+        S = max(1, min(S, steps - 1))
     t0 = time.perf_counter()
-    orc.run2d(U, n, n, 2, 1 / n, 1 / n, 1.4, 0.4, nsteps=S, bc=BC_OUTFLOW)
+    dts += list(run(S)[2])
     el = time.perf_counter() - t0
-    return {"value": n * n * 2 * S / el, "unit": UNIT, "cores": th, "kind": "port",
+    base = {"value": n * n * 2 * S / el, "unit": UNIT, "cores": th, "kind": "port",
             "sample": f"{S} RK2 steps (after 1 untimed) of the {n}x{n} FP64 diagonal Riemann problem, "
                       f"oracle/euler_oracle.c with OpenMP ({th} threads), {el:.1f} s"}
+    if final_f64 is None:
+        return base, None
+    Ug, tg, kg = final_f64
+    rest = steps - 1 - S
+    if rest > 0:
+        dts += list(run(rest)[2])
+    tc = 0.0
+    for d in dts:  # the solver's clock: time += dt each step
+        tc += d
+    a, b = Ug[:, 2:-2, 2:-2], U[:, 2:-2, 2:-2]
+    diff = np.abs(a - b)
+    rel = diff / np.maximum(np.abs(b), 1e-300)
+    parity = {"steps": len(dts), "gpu_steps": int(kg), "bit_exact": bool(np.array_equal(a, b)),
+              "max_rel_diff": float(rel.max()), "max_abs_diff": float(diff.max()),
+              "time_gpu": float(tg), "time_oracle": tc, "time_equal": bool(tg == tc),
+              "oracle": f"oracle/euler_oracle.c, {th} threads, {len(dts)} steps from the initial state"}
+    return base, parity
 
 
 def run_reference(args, rank):
@@ -759,7 +844,7 @@ def run_reference(args, rank):
     first nx_s rows of the n x n grid as an outflow domain -- sized from the
     warm-up timing so the whole run stays within minutes."""
     from oracle.oracle import BC_OUTFLOW, Oracle
-    from nest_b200.problems import riemann_2d
+    riemann_2d = load_problems().riemann_2d
     orc = Oracle()
     th = host_threads()
     orc.set_threads(th)
@@ -781,13 +866,11 @@ def run_reference(args, rank):
     value = nx_s * n * 2 * args.steps / el
     sample = (f"{args.steps} RK2 steps of a {nx_s}x{n} slab of the {n}x{n} FP64 diagonal Riemann problem, "
               f"oracle/euler_oracle.c (the scheme's CPU restatement; nest has no 2D RK2), OpenMP {th} threads")
-    head = args.forms.split(",")[0].strip()
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"riemann2d {n}x{n} {head}", "nx": n, "ny": n, "bc": "outflow", "cfl": 0.4,
-                   "gamma": 1.4},
+        "config": workload_config(n, 1, "f64", False),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

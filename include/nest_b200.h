@@ -28,8 +28,11 @@ typedef enum nest_status {
     NEST_ERR_INVALID = 1,     /* bad argument or handle */
     NEST_ERR_CUDA = 2,        /* a CUDA runtime call failed */
     NEST_ERR_OOM = 3,         /* device allocation failed */
-    NEST_ERR_NUMERIC = 4,     /* non-finite wave speed (state blew up) */
-    NEST_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+    NEST_ERR_NUMERIC = 4,     /* after a step: rho <= 0 or p <= 0 in an interior cell (nest's
+                                 positivity check, examples/sod1d/sod1d.cpp:279-301, here after
+                                 every step), or a NaN / Inf state; nest_last_error() names the
+                                 step and the first failing cell.  The solver stops at that step
+                                 (later steps are no-ops) until a new state is uploaded. */
     NEST_ERR_UNSUPPORTED = 6  /* valid request this build does not implement */
 } nest_status;
 
@@ -265,10 +268,10 @@ nest_status nest_adjoint_stats(nest_adjoint* a, double* fwd_ms, double* bwd_ms, 
 /* control block) is a fixed array inside the library, so this call makes   */
 /* no cudaMalloc / cudaFree.  The array holds n_interior + 2*n_halo <=      */
 /* NEST_NOALLOC_MAX_CELLS cells (about 1.6 MB, held by every GPU that loads */
-/* the library until exit); larger sizes return NEST_ERR_INVALID.  The      */
-/* first call on a device looks up the array's device address, so make it   */
-/* before any stream capture.  All calls share the array: calls that        */
-/* overlap on the GPU race.                                                 */
+/* the library until exit); larger sizes return NEST_ERR_INVALID.  Every    */
+/* call looks up the array's address in the current device's context and    */
+/* waits for its stream (it reads the step count back every 32 steps).      */
+/* All calls share the array: calls that overlap on the GPU race.           */
 /*                                                                          */
 /* d_state: device SoA [var * n_total + i], n_total = n_interior + 2 n_halo */
 /* (nest's layout), advanced in place from time 0 to t_final with CFL dt,   */

@@ -16,7 +16,7 @@ NEST_OK = 0
 NEST_ERR_INVALID = 1
 STATUS_NAMES = {
     0: "NEST_OK", 1: "NEST_ERR_INVALID", 2: "NEST_ERR_CUDA", 3: "NEST_ERR_OOM",
-    4: "NEST_ERR_NUMERIC", 5: "NEST_ERR_TIMEOUT", 6: "NEST_ERR_UNSUPPORTED",
+    4: "NEST_ERR_NUMERIC", 6: "NEST_ERR_UNSUPPORTED",
 }
 BC_PERIODIC, BC_OUTFLOW = 0, 1
 F64, F32 = 0, 1

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -47,6 +48,20 @@ double nestb::rt::bits_to_double(unsigned long long b) {
 }
 
 nest_status nestb::record_error(nest_status st, const std::string& msg) { return fail(st, msg); }
+
+std::string nestb::ctrl_error_text(const StepCtrl& c, int steps_now) {
+    char buf[256];
+    if (c.bad_step > 0) {
+        // the recorded cell names the failure: a NaN is a non-finite state
+        const bool nan = !(c.bad_rho == c.bad_rho) || !(c.bad_p == c.bad_p);
+        std::snprintf(buf, sizeof buf, "%s at step %d in cell (%d, %d): rho = %.17g, p = %.17g",
+                      nan ? "non-finite state (NaN)" : "positivity violation (rho <= 0 or p <= 0)", c.bad_step,
+                      c.bad_i, c.bad_j, c.bad_rho, c.bad_p);
+    } else {
+        std::snprintf(buf, sizeof buf, "non-finite state: infinite or NaN wave speed after step %d", steps_now);
+    }
+    return buf;
+}
 
 namespace {
 
@@ -151,7 +166,8 @@ nest_status enqueue_steps(nest_solver* s, int nsteps, const LoopParams& lp) {
 nest_status nestb::rt::read_ctrl(nest_solver* s) {
     CK(cudaMemcpyAsync(s->host_ctrl, s->ctrl, sizeof(StepCtrl), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
-    if (s->host_ctrl->err & ERRW_NONFINITE) return fail(NEST_ERR_NUMERIC, "non-finite wave speed: the state blew up");
+    if (s->host_ctrl->err & ERRW_STOP)
+        return fail(NEST_ERR_NUMERIC, ctrl_error_text(*s->host_ctrl, s->host_ctrl->step[s->parity]));
     return NEST_OK;
 }
 
@@ -320,6 +336,8 @@ static nest_status upload_impl(nest_solver* s, const void* src, int layout, cuda
     if (!src) return fail(NEST_ERR_INVALID, "null source");
     r = copy_state(s, nullptr, src, layout, true, kind);
     if (r != NEST_OK) return r;
+    // a new state starts without an error record
+    CK(cudaMemsetAsync(&s->ctrl->err, 0, sizeof(StepCtrl) - offsetof(StepCtrl, err), s->st));
     r = prepare(s);
     if (r != NEST_OK) return r;
     CK(cudaStreamSynchronize(s->st));
@@ -920,7 +938,10 @@ nest_status nest_batch_upload(nest_batch* b, int problem, const void* host, int 
     nest_status r = batch_check(b);
     if (r != NEST_OK) return r;
     if (!host) return fail(NEST_ERR_INVALID, "null source");
+    if (problem < 0 || problem >= b->count) return fail(NEST_ERR_INVALID, "problem index out of range");
     b->prepared = false;
+    // a new state starts without an error record
+    CK(cudaMemsetAsync(&b->ctrls[problem].err, 0, sizeof(StepCtrl) - offsetof(StepCtrl, err), b->st));
     return batch_copy(b, problem, nullptr, host, layout, true);
 }
 
@@ -1024,7 +1045,9 @@ nest_status nest_batch_times(nest_batch* b, double* times, int* steps) {
     CK(cudaMemcpyAsync(b->host_ctrls, b->ctrls, sizeof(StepCtrl) * b->count, cudaMemcpyDeviceToHost, b->st));
     CK(cudaStreamSynchronize(b->st));
     for (int p = 0; p < b->count; ++p) {
-        if (b->host_ctrls[p].err & ERRW_NONFINITE) return fail(NEST_ERR_NUMERIC, "non-finite wave speed in problem " + std::to_string(p));
+        if (b->host_ctrls[p].err & ERRW_STOP)
+            return fail(NEST_ERR_NUMERIC, "problem " + std::to_string(p) + ": " +
+                                              ctrl_error_text(b->host_ctrls[p], b->host_ctrls[p].step[b->parity]));
         if (times) times[p] = b->host_ctrls[p].time[b->parity];
         if (steps) steps[p] = b->host_ctrls[p].step[b->parity];
     }

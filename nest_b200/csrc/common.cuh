@@ -20,13 +20,14 @@ namespace nestb {
 // Boundary conditions on the domain edges.
 enum { BC_PERIODIC = 0, BC_OUTFLOW = 1 };
 
-// Device error word bits (read back by the host after a run).
+// Device error word bits (read back by the host after a run).  A step that
+// starts with either bit set does not run: the state stays as the failing
+// step left it.
 enum : unsigned {
-    ERRW_NONFINITE = 1u,   // a wave speed was NaN/Inf
-    ERRW_NONPOSITIVE = 2u, // rho or p below zero after the update (FP64 form)
-    ERRW_TIMEOUT = 4u,     // a bounded spin gave up
-    ERRW_REPAIRED = 8u,    // FP32 form: positivity repair was applied
+    ERRW_NONFINITE = 1u,   // a wave speed, density or pressure was NaN / Inf
+    ERRW_NONPOSITIVE = 2u, // rho <= 0 or p <= 0 in an interior cell after a step
 };
+constexpr unsigned ERRW_STOP = ERRW_NONFINITE | ERRW_NONPOSITIVE;
 
 // Per-solver control block in device memory.  Fields indexed [p] belong to
 // the step launched with parity p; a step with parity p reads slot p and
@@ -37,8 +38,13 @@ struct StepCtrl {
     unsigned long long maxs[2][2];  // [p][axis] max wave speed of U at the start of step p (bits of a non-negative double)
     int step[2];                    // completed steps at the start of the step
     int active[2];                  // stage 1 sets it: 1 = the step runs, 0 = finished
-    unsigned err;                   // ERRW_* bits
     unsigned repairs;               // FP32 form: number of repaired cells
+    // error record (cleared by an upload; the fields from `err` on)
+    unsigned err;                   // ERRW_* bits
+    int bad_step;                   // first failing cell: steps completed when it was found (0: none recorded),
+    int bad_i, bad_j;               // its interior index (1D: bad_j = 0)
+    int pad_;
+    double bad_rho, bad_p;          // and its density and pressure
 };
 
 // Time-loop parameters shared by all launches of a solver.
@@ -86,9 +92,27 @@ __device__ __forceinline__ T warp_sum(T v) {
     return v;
 }
 
+// nest's positivity check (examples/sod1d/sod1d.cpp:279-301: rho <= 0 or
+// p <= 0 in an interior cell is an error) runs on every cell after every
+// step (nest: every 10th step).  The kernels test !(rho > 0) || !(p > 0),
+// which a NaN fails too, and call this on the rare failing path: the bit is
+// ERRW_NONFINITE for a NaN, else ERRW_NONPOSITIVE, and the first failing
+// cell records the step (`step_done` = steps completed, this one included),
+// its interior index and its values.
+__device__ __forceinline__ void flag_cell(StepCtrl* c, int step_done, double rho, double pr, int i, int j) {
+    const unsigned bit = (rho == rho && pr == pr) ? ERRW_NONPOSITIVE : ERRW_NONFINITE;
+    if (atomicOr(&c->err, bit) & ERRW_STOP) return;  // an earlier cell holds the record
+    c->bad_step = step_done;
+    c->bad_i = i;
+    c->bad_j = j;
+    c->bad_rho = rho;
+    c->bad_p = pr;
+}
+
 // Decide the step: returns false when the run is finished.  Every block of
 // stage 1 evaluates this on the same inputs, so all agree; block 0 publishes.
 __device__ __forceinline__ bool step_is_done(const StepCtrl* c, int p, const LoopParams& lp) {
+    if (c->err & ERRW_STOP) return true;
     double t = c->time[p];
     int s = c->step[p];
     if (lp.t_final > 0.0 && !(t < lp.t_final)) return true;

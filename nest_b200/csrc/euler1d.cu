@@ -82,8 +82,10 @@ k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int
         Wd[x] = r; Wd[nt + x] = u; Wd[2 * nt + x] = pr;
         ghost_copies_1d(Wd, nt, n, h, bc, c, r, u, pr);
     };
-    // max |u| + c over this thread's cells of A (benchmark_euler1d.cpp:168-180), warp maxima to red
-    auto speeds = [&]() {
+    // max |u| + c over this thread's cells of A (benchmark_euler1d.cpp:168-180), warp maxima to red.
+    // step_done > 0: the state after that step, checked for positivity; a
+    // failing cell makes the maximum infinite, which ends the loop for the CTA
+    auto speeds = [&](int step_done) {
         double ms = 0.0;
 #pragma unroll
         for (int q = 0; q < K; ++q) {
@@ -93,6 +95,10 @@ k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int
                 const double u = W[nt + x], pr = W[2 * nt + x], r = W[x];
                 const double cs = sqrt(gamma * pr / r);
                 ms = smax(ms, fabs(u) + cs);
+                if (step_done > 0 && (!(r > 0.0) || !(pr > 0.0))) {
+                    flag_cell(ctrl, step_done, r, pr, c, 0);
+                    ms = __longlong_as_double(0x7ff0000000000000ll);
+                }
             }
         }
         ms = warp_max(ms);
@@ -161,13 +167,15 @@ k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int
         }
     }
     __syncthreads();
-    speeds();
+    speeds(0);
     __syncthreads();
     double ms = reduce_red();
 
     double time = ctrl->time[p];
     int step = ctrl->step[p];
+    const bool stopped = (ctrl->err & ERRW_STOP) != 0;  // an earlier step failed: run nothing
     for (int it = 0;; ++it) {
+        if (stopped) break;
         if (lp.step_budget > 0 && it >= lp.step_budget) break;
         if (lp.t_final > 0.0 && !(time < lp.t_final)) break;
         if (lp.max_steps > 0 && step >= lp.max_steps) break;
@@ -191,7 +199,7 @@ k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int
         faces();                        // stage 2 fluxes
         __syncthreads();
         update(U1, U, true, dtdx);      // U = (U + U1 - dt L(U1)) / 2, W = prims(U), ghosts
-        speeds();
+        speeds(step + 1);
         __syncthreads();
         ms = reduce_red();
         time += dt;
@@ -314,8 +322,10 @@ k1d_cluster(double* __restrict__ Ug, int n, int h, int m, double dx, double gamm
         }
     };
     // stage update of this CTA's cells; in stage 2 (heun) also the max |u|+c
-    // of the new state (same formulas as `speeds`) into red
-    auto update = [&](const double* Uin, double* Uout, bool heun, double dtdx, int bnext) {
+    // of the new state (same formulas as `speeds`) into red and the
+    // positivity check of step `step_done`: a failing cell makes the maximum
+    // infinite, which ends the loop on every CTA of the cluster
+    auto update = [&](const double* Uin, double* Uout, bool heun, double dtdx, int bnext, int step_done) {
         double ms = 0.0;
         for (int l = tid; l < mloc; l += T) {
             double v[3];
@@ -331,6 +341,10 @@ k1d_cluster(double* __restrict__ Ug, int n, int h, int m, double dx, double gamm
                 const double rr = w[2 + l], u = w[mw + 2 + l], pr = w[2 * mw + 2 + l];
                 const double cs = sqrt(gamma * pr / rr);
                 ms = smax(ms, fabs(u) + cs);
+                if (!(rr > 0.0) || !(pr > 0.0)) {
+                    flag_cell(ctrl, step_done, rr, pr, c_lo + l, 0);
+                    ms = __longlong_as_double(0x7ff0000000000000ll);
+                }
             }
         }
         if (heun) {
@@ -353,7 +367,9 @@ k1d_cluster(double* __restrict__ Ug, int n, int h, int m, double dx, double gamm
 
     double time = ctrl->time[p];
     int step = ctrl->step[p];
+    const bool stopped = (ctrl->err & ERRW_STOP) != 0;  // an earlier step failed: run nothing
     for (int it = 0;; ++it) {
+        if (stopped) break;
         if (lp.step_budget > 0 && it >= lp.step_budget) break;
         if (lp.t_final > 0.0 && !(time < lp.t_final)) break;
         if (lp.max_steps > 0 && step >= lp.max_steps) break;
@@ -375,11 +391,11 @@ k1d_cluster(double* __restrict__ Ug, int n, int h, int m, double dx, double gamm
         if (r == 0 && tid == 0 && lp.dts_out && step < lp.dts_cap) lp.dts_out[step] = dt;
         const double dtdx = dt / dx;
         __syncthreads();                // stage 1 fluxes (from W0 = prims(U)) complete
-        update(U, U1, false, dtdx, 1);  // U1, W1 = prims(U1) and the neighbours' halos
+        update(U, U1, false, dtdx, 1, 0);  // U1, W1 = prims(U1) and the neighbours' halos
         cl.sync();
         faces(1);                       // stage 2 fluxes
         __syncthreads();
-        update(U1, U, true, dtdx, 0);   // U = (U + U1 - dt L(U1)) / 2, W0 = prims(U), max |u|+c
+        update(U1, U, true, dtdx, 0, step + 1);  // U = (U + U1 - dt L(U1)) / 2, W0 = prims(U), max |u|+c
         cl.sync();
         time += dt;
         ++step;

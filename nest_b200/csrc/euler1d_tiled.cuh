@@ -24,11 +24,12 @@ constexpr int T1 = 256;       // cells per tile
 // full warps)
 constexpr int NT1 = T1 + 32;
 
-// Max |u|+c of one cell (benchmark_euler1d.cpp:170-178).
+// Max |u|+c of one cell (benchmark_euler1d.cpp:170-178); p receives the
+// cell's pressure (eos_t::pressure, clamped at 0) for the positivity check.
 template <typename T>
-__device__ __forceinline__ T cell_speed_1d(T rho, T mom, T erg, T gamma, T gm1) {
+__device__ __forceinline__ T cell_speed_1d(T rho, T mom, T erg, T gamma, T gm1, T& p) {
     T u = mom / rho;
-    T p = eos_pressure(gm1, rho, mom, erg);
+    p = eos_pressure(gm1, rho, mom, erg);
     T c = sqrt(gamma * p / rho);
     return fabs(u) + c;
 }
@@ -112,7 +113,11 @@ k1d_stage(const T* __restrict__ Uin, const T* Un, T* Uout,
             Uout[k * nt + e] = v[k];
             push_ghosts_1d(Uout, nt, k, c, n, h, bc, v[k]);
         }
-        if (STAGE == 2) ms = (double)cell_speed_1d(v[0], v[1], v[2], gamma, gm1);
+        if (STAGE == 2) {
+            T pr;
+            ms = (double)cell_speed_1d(v[0], v[1], v[2], gamma, gm1, pr);
+            if (!(v[0] > T(0)) || !(pr > T(0))) flag_cell(ctrl, ctrl->step[p] + 1, (double)v[0], (double)pr, c, 0);
+        }
     }
     if (STAGE == 2) {
         ms = warp_max(ms);
@@ -147,7 +152,8 @@ k1d_prepare(T* U, int n, int h, double gamma_d, int bc, StepCtrl* ctrl, int p) {
         push_ghosts_1d(U, nt, 0, c, n, h, bc, v0);
         push_ghosts_1d(U, nt, 1, c, n, h, bc, v1);
         push_ghosts_1d(U, nt, 2, c, n, h, bc, v2);
-        ms = (double)cell_speed_1d(v0, v1, v2, gamma, gm1);
+        T pr;
+        ms = (double)cell_speed_1d(v0, v1, v2, gamma, gm1, pr);
     }
     ms = warp_max(ms);
     int w = threadIdx.x >> 5, l = threadIdx.x & 31;

@@ -417,6 +417,14 @@ __device__ __forceinline__ void x2_body(const A& a, int strip, int tile_row) {
                         pr = mul2(sp(gm1), sub2(s.d, ke));
                     }
                 }
+                {
+                    // positivity (with REPAIR: NaN only, the repair keeps rho and p positive in FP64)
+                    const bool bx = REPAIR ? (!(s.a.x == s.a.x) || !(pr.x == pr.x)) : (!(s.a.x > 0.f) || !(pr.x > 0.f));
+                    const bool by = out_b && (REPAIR ? (!(s.a.y == s.a.y) || !(pr.y == pr.y))
+                                                     : (!(s.a.y > 0.f) || !(pr.y > 0.f)));
+                    if (bx) flag_cell(a.ctrl, a.ctrl->step[a.p] + 1, s.a.x, pr.x, i, ca);
+                    if (by) flag_cell(a.ctrl, a.ctrl->step[a.p] + 1, s.a.y, pr.y, i, ca + 1);
+                }
                 F2 pp = max2(pr, 1e-10f);
                 F2 gp = mul2(sp(gamma), pp);
                 F2 c = mul2(gp, rsq2(mul2(gp, rho)));

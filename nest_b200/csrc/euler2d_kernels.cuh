@@ -143,9 +143,12 @@ __device__ __forceinline__ void hlle4(T gamma, T gm1, T igm1,
 }
 
 // Wave speeds |u|+c, |v|+c of a conserved state with the 1e-10 floors of
-// compute_dt_2d (examples/sod2d/euler2d.hpp:254-263).
+// compute_dt_2d (examples/sod2d/euler2d.hpp:254-263).  Returns the pressure
+// of cons2prim before its clamp, (gamma-1) (E - ke2(rho, u, v)), for the
+// positivity check: for rho >= 1e-10 (no floor) u and v are cons2prim's, so
+// this is the scheme's own pressure.
 template <typename T>
-__device__ __forceinline__ void cell_speeds(T U0, T U1, T U2, T U3, T gamma, T gm1, T& sx, T& sy) {
+__device__ __forceinline__ T cell_speeds_p(T U0, T U1, T U2, T U3, T gamma, T gm1, T& sx, T& sy) {
     T rho = smax(U0, T(1e-10));
     T u, v;
     if (Pol<T>::exact) {
@@ -161,6 +164,12 @@ __device__ __forceinline__ void cell_speeds(T U0, T U1, T U2, T U3, T gamma, T g
     T c = Pol<T>::sound(gamma, p, rho);
     sx = fabs(u) + c;
     sy = fabs(v) + c;
+    return gm1 * (U3 - ke2(rho, u, v));
+}
+
+template <typename T>
+__device__ __forceinline__ void cell_speeds(T U0, T U1, T U2, T U3, T gamma, T gm1, T& sx, T& sy) {
+    (void)cell_speeds_p<T>(U0, U1, U2, U3, gamma, gm1, sx, sy);
 }
 
 // dt = cfl * min(dx / max(|u|+c), dy / max(|v|+c)), euler2d.hpp:249-270.
@@ -358,7 +367,17 @@ __device__ __forceinline__ void stage2d_body(const StageArgs<T>& a, int strip, i
                             }
                         }
                         T sx, syv;
-                        cell_speeds<T>(s0, s1, s2, s3, gamma, gm1, sx, syv);
+                        const T pc = cell_speeds_p<T>(s0, s1, s2, s3, gamma, gm1, sx, syv);
+                        // positivity (REPAIR: NaN only, the repair keeps rho and p positive in FP64)
+                        if (REPAIR ? (!(s0 == s0) || !(pc == pc)) : (!(s0 >= T(1e-10)) || !(pc > T(0)))) {
+                            T pe = pc;
+                            if (s0 > T(0) && s0 < T(1e-10)) {  // rho under the speed floor: unfloored pressure
+                                T ue = Pol<T>::div(s1, s0), ve = Pol<T>::div(s2, s0);
+                                pe = gm1 * (s3 - ke2(s0, ue, ve));
+                            }
+                            if (!(s0 > T(0)) || !(pe > T(0)) || !(pe == pe))
+                                flag_cell(a.ctrl, a.ctrl->step[a.p] + 1, (double)s0, (double)pe, i, j);
+                        }
                         smx = smax(smx, (double)sx);
                         smy = smax(smy, (double)syv);
                         tot0 += (double)s0; tot1 += (double)s1; tot2 += (double)s2; tot3 += (double)s3;

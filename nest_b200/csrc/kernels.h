@@ -84,6 +84,11 @@ cudaError_t launch_sum_batch(const double* partials, const int* first, int count
 
 // Records msg as the calling thread's last error (read by nest_last_error()).
 nest_status record_error(nest_status st, const std::string& msg);
+// Text of the error record of a control block whose err word is set:
+// positivity violation or non-finite state, with the step and the first
+// failing cell when one was recorded (`steps_now`: the solver's step count,
+// used when no cell was).
+std::string ctrl_error_text(const StepCtrl& c, int steps_now);
 
 // Fixed-order sum of per-warp totals (deterministic).
 cudaError_t launch_sum_partials(const double* partials, long long nrec, double* out4, cudaStream_t st);

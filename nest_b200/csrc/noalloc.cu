@@ -17,7 +17,6 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "../../include/nest_b200.h"
@@ -37,28 +36,20 @@ struct NoallocScratch {
 
 static __device__ __align__(256) NoallocScratch g_noalloc_scratch;
 
-constexpr int MAX_DEVICES = 64;
-std::mutex g_setup_mutex;
-NoallocScratch* g_scratch_addr[MAX_DEVICES] = {};
-
 nest_status noalloc_fail(nest_status st, const std::string& msg) { return nestb::record_error(st, msg); }
 
-// Device address of the scratch array on the current device.  The first call
-// on a device looks it up (with that device current) and caches it.
+// Device address of the scratch array in the current device's context.  In
+// host code the array's name is only a host-side stand-in; the address comes
+// from cudaGetSymbolAddress with the device current.  It is looked up on every
+// call (a host-side table lookup once the module is loaded), so a device reset
+// or another context, which can place the array elsewhere, never leaves a
+// stale address behind.
 nest_status scratch_for_current_device(NoallocScratch** out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return noalloc_fail(NEST_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= MAX_DEVICES) return noalloc_fail(NEST_ERR_UNSUPPORTED, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return noalloc_fail(NEST_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratch_addr[dev] = static_cast<NoallocScratch*>(p);
-    }
-    *out = g_scratch_addr[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return noalloc_fail(NEST_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    *out = static_cast<NoallocScratch*>(p);
     return NEST_OK;
 }
 
@@ -100,7 +91,8 @@ extern "C" nest_status nest_euler1d_run_noalloc(double* d_state, int n_interior,
         if (e == cudaSuccess) e = cudaMemcpyAsync(&host, ctrl, sizeof host, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) break;
-        if (host.err & nestb::ERRW_NONFINITE) return noalloc_fail(NEST_ERR_NUMERIC, "non-finite wave speed");
+        if (host.err & nestb::ERRW_STOP)
+            return noalloc_fail(NEST_ERR_NUMERIC, nestb::ctrl_error_text(host, host.step[parity]));
         if (!(host.time[parity] < t_final)) break;
         if (host.step[parity] == last_step) return noalloc_fail(NEST_ERR_NUMERIC, "time stopped advancing");
         last_step = host.step[parity];

@@ -30,11 +30,21 @@ def _ptr(a: np.ndarray | None):
     return a.ctypes.data_as(_dp)
 
 
+# Where the nest source tree is looked for when NEST_REF is not set.
+DEFAULT_REF = "/root/reference"
+
+
 def build(quiet: bool = True) -> None:
-    """Run oracle/Makefile (the system gcc-13 with OpenMP)."""
+    """Run oracle/Makefile (the system gcc-13 with OpenMP); nest's own sources
+    are compiled into _ref/ when their tree is present (environment variable
+    NEST_REF, else DEFAULT_REF)."""
     import subprocess
 
-    out = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+    ref = os.environ.get("NEST_REF", DEFAULT_REF)
+    cmd = ["make", "-C", str(HERE)]
+    if Path(ref, "examples", "sod1d", "euler1d.hpp").exists():
+        cmd.append(f"REF={ref}")
+    out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:

@@ -56,6 +56,29 @@ def test_fp64_run_to_t_final(gpu, oracle):
     assert np.array_equal(got[:, 2:-2, 2:-2], want[:, 2:-2, 2:-2])
 
 
+def test_fp64_full_size_matches_oracle(gpu, oracle):
+    """The benchmark workload itself (diagonal Riemann problem, 4096^2 as 16 x
+    16 patches of 256^2, outflow, CFL 0.4, 200 RK2 steps) through
+    nest_solver_step with the default launch shape: every cell of all four
+    variables and the simulated time equal the oracle's bit for bit (the
+    tolerance `north_star` allows is a relative 1e-12; the FP64 form has no
+    FMA contraction, so it is exact).  The oracle runs on every host core."""
+    import os
+    n, steps = 4096, 200
+    U = riemann_2d(n, n)
+    s, got = gpu_run(gpu, U, n, n, (BC_OUTFLOW, BC_OUTFLOW), nsteps=steps)
+    t_gpu, k = s.time()
+    s.close()
+    oracle.set_threads(len(os.sched_getaffinity(0)))
+    want = np.ascontiguousarray(U)
+    ksteps, t, _ = oracle.run2d(want, n, n, 2, 1 / n, 1 / n, G, 0.4, nsteps=steps, bc=BC_OUTFLOW)
+    a, b = got[:, 2:-2, 2:-2], want[:, 2:-2, 2:-2]
+    rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+    assert rel.max() <= 1e-12, rel.max()
+    assert np.array_equal(a, b)
+    assert k == ksteps == steps and t_gpu == t
+
+
 def test_fp64_full_size_mirror_symmetry(gpu):
     """Diagonal Riemann problem, 4096^2, 200 steps (the benchmark workload):
     the scheme is mirror symmetric about x = y, so rho(i,j) == rho(j,i) and
