@@ -14,6 +14,10 @@ LIB_PATH = Path(os.environ.get("NEST_B200_LIB", PKG / "lib" / "libnest_b200.so")
 
 NEST_OK = 0
 NEST_ERR_INVALID = 1
+NEST_ERR_CUDA = 2
+NEST_ERR_OOM = 3
+NEST_ERR_NUMERIC = 4
+NEST_ERR_UNSUPPORTED = 6
 STATUS_NAMES = {
     0: "NEST_OK", 1: "NEST_ERR_INVALID", 2: "NEST_ERR_CUDA", 3: "NEST_ERR_OOM",
     4: "NEST_ERR_NUMERIC", 6: "NEST_ERR_UNSUPPORTED",
