@@ -233,6 +233,57 @@ nest_status nest_exchange_layout(nest_exchange* x, long long* offsets, int* boxe
 nest_status nest_exchange_execute(nest_exchange* x, void* d_data, int precision, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Device pipeline executor over nest's per-patch storage (FP64).           */
+/* Replaces nest's pipeline_t / execute (include/nest/pipeline.hpp:14-151)  */
+/* and the host stage loops of examples/sod1d/sod1d.cpp:219-302: a pipeline */
+/* is a list of stages, each one launch over every patch; execute() runs    */
+/* them once in order, run() repeats them until time >= t_final with the   */
+/* steps replayed from CUDA graphs.  The storage is the exchange plan's     */
+/* (nest_pipeline_plan: patches one after another, nvars SoA planes over    */
+/* each patch's extended space).  Buffers: 0 = the caller's device state,   */
+/* 1..nwork = work arrays the pipeline owns, of the same layout.            */
+/*   EXCHANGE   halos of buffer src (nest's fill_all_halos)                 */
+/*   EULER_RHS  compute: dst = src - (dt/dx) (F_{i+1/2} - F_{i-1/2}) on the */
+/*              interiors, nest's euler_rhs_t (examples/sod1d/euler1d.hpp:  */
+/*              279-397) with its one-sided patch edges; 1D                 */
+/*   COPY       compute: dst = src on the interiors                         */
+/*   AVERAGE    compute: dst = 0.5 src + 0.5 aux on the interiors           */
+/*   CFL_DT     reduce: init 0, max |u| + c over each interior of src,      */
+/*              finalize dt = param * dx / max, clipped to t_final - time   */
+/*              (compute_dt, sod1d.cpp:97-128); during run() a step that    */
+/*              starts at or past t_final does nothing; 1D                  */
+/*   CHECK      nest's positivity check (sod1d.cpp:279-301) of src when the */
+/*              step in progress is a multiple of param; place it before    */
+/*              CLOCK; failures surface as NEST_ERR_NUMERIC; 1D             */
+/*   CLOCK      time += dt, step += 1                                       */
+/* dt, time and the step count stay on the device (nest_pipeline_clock).   */
+/* ------------------------------------------------------------------------ */
+enum {
+    NEST_STAGE_EXCHANGE = 1, NEST_STAGE_EULER_RHS = 2, NEST_STAGE_COPY = 3, NEST_STAGE_AVERAGE = 4,
+    NEST_STAGE_CFL_DT = 5, NEST_STAGE_CHECK = 6, NEST_STAGE_CLOCK = 7
+};
+typedef struct nest_pipeline nest_pipeline;
+/* Patch grid as nest_exchange_create_periodic; limiter 0 minmod, 1 MC, 2 none
+ * (limiter_t, euler1d.hpp:106-137); nwork work buffers (0..16). */
+nest_status nest_pipeline_create(int dim, int nx, int ny, int npx, int npy, int halo, double dx, double gamma,
+                                 int limiter, int nwork, nest_pipeline** out);
+nest_status nest_pipeline_destroy(nest_pipeline* p);
+/* The pipeline's exchange plan (layout queries; owned by the pipeline). */
+nest_status nest_pipeline_plan(nest_pipeline* p, nest_exchange** plan);
+nest_status nest_pipeline_add(nest_pipeline* p, int kind, int src, int dst, int aux, double param);
+/* All stages once, in order, enqueued on `stream` (NULL: the pipeline's own). */
+nest_status nest_pipeline_execute(nest_pipeline* p, void* d_state, void* stream);
+/* Execute until time >= t_final (needs a CFL_DT stage) or max_steps (> 0)
+ * more steps; waits.  *steps_out = steps taken. */
+nest_status nest_pipeline_run(nest_pipeline* p, void* d_state, double t_final, int max_steps, int* steps_out,
+                              void* stream);
+/* Clock (waits; NEST_ERR_NUMERIC after a failed CHECK). */
+nest_status nest_pipeline_clock(nest_pipeline* p, double* time, double* dt, int* step);
+nest_status nest_pipeline_set_clock(nest_pipeline* p, double time, double dt, int step);
+/* Device address of work buffer `index` (1..nwork). */
+nest_status nest_pipeline_buffer(nest_pipeline* p, int index, void** dev);
+
+/* ------------------------------------------------------------------------ */
 /* Discrete adjoint with checkpointing.  No counterpart in nest.            */
 /* The forward sweep runs the solver from its current state for nsteps with */
 /* CFL dt (recorded) or a given dt sequence; the backward sweep maps the    */

@@ -9,10 +9,11 @@ from ._capi import (BC_OUTFLOW, BC_PERIODIC, F32, F64, FLAG_FP32_SCALAR, FLAG_LI
                     FLAG_TOTALS, LAYOUT_EXTENDED, LAYOUT_INTERIOR, LIB_PATH, NestError)
 from .batch import Batch
 from .exchange import PeriodicExchange
+from .pipeline import Pipeline, sod1d_pipeline
 from .solver import Euler1DGPU, Solver
 
 __all__ = [
-    "Batch", "PeriodicExchange", "Euler1DGPU", "Solver", "NestError", "BC_PERIODIC", "BC_OUTFLOW", "F64", "F32",
+    "Batch", "PeriodicExchange", "Pipeline", "sod1d_pipeline", "Euler1DGPU", "Solver", "NestError", "BC_PERIODIC", "BC_OUTFLOW", "F64", "F32",
     "LAYOUT_EXTENDED", "LAYOUT_INTERIOR", "FLAG_TOTALS", "FLAG_REPAIR", "FLAG_NO_RESIDENT", "FLAG_FP32_SCALAR", "FLAG_SPLIT_COMPAT",
     "FLAG_LIMITER_MC", "FLAG_LIMITER_NONE",
     "LIB_PATH",

@@ -43,6 +43,7 @@ UNITS = {
     "adjoint2d_f32x2.cu": ["-use_fast_math"],
     "adjoint2d_f64rm.cu": ["-fmad=false"],
     "datio.cpp": ["-x", "cu", "-Xcompiler", "-ffp-contract=off"],
+    "pipeline.cu": ["-fmad=false"],
 }
 
 

@@ -219,6 +219,7 @@ class Reference:
             "ref_run_cpu_sod": (None, [i, d, d, _dp]),
             "ref_write_sod1d": (None, [_dp, i, i, i, d, d, d, d, i]),
             "ref_write_sod2d": (None, [_dp, i, i, i, i, d, d, d, d, d, d, i]),
+            "ref_pipeline_euler1d": (None, [_dp, i, i, i, d, d, i, i, _dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -262,6 +263,15 @@ class Reference:
         Uout = np.zeros_like(Uin)
         self.L.ref_patch_stage(_ptr(np.ascontiguousarray(Uin)), _ptr(Uout), n, h, dx, dt, gamma)
         return Uout
+
+    def pipeline_euler1d(self, U, npatch, halo, gamma, cfl, nexec, limiter=0):
+        """nest::execute of (dt reduce, exchange, euler_rhs compute) on nest's
+        patches, nexec times, from the global interior state U [3][n];
+        returns (final U, dts)."""
+        U = np.ascontiguousarray(U, np.float64).copy()
+        dts = np.zeros(nexec)
+        self.L.ref_pipeline_euler1d(_ptr(U), U.shape[1], npatch, halo, gamma, cfl, limiter, nexec, _ptr(dts))
+        return U, dts
 
     def benchmark_cpu(self, n_zones, t_final):
         steps = C.c_int(0)

@@ -224,3 +224,34 @@ def test_sod2d_example_golden(oracle, ref):
     assert abs(t - 0.2) < 1e-15
     assert np.allclose(rho, g["rho"], rtol=2e-10, atol=0)
     assert np.allclose(u, g["u"], rtol=2e-10, atol=1e-14)
+
+
+def test_nest_pipeline_program_equals_oracle_patch_steps(oracle, ref):
+    """nest::execute of (dt reduce, exchange, euler_rhs compute) on nest's own
+    patches (oracle/ref_prog_pipeline.cpp) equals forward-Euler steps of the
+    oracle's patch stage with the periodic exchange: pins the program the
+    device pipeline is compared with."""
+    n, npatch, h, nexec, cfl = 403, 5, 2, 12, 0.4
+    rng = np.random.default_rng(3)
+    x = (np.arange(n) + 0.5) / n
+    rho = np.where(x < 0.5, 1.0, 0.125) + 0.01 * rng.random(n)
+    u = 0.2 * np.sin(2 * np.pi * x)
+    p = np.where(x < 0.5, 1.0, 0.1)
+    U = np.stack([rho, rho * u, p / 0.4 + 0.5 * rho * u * u])
+    got, dts = ref.pipeline_euler1d(U, npatch, h, G, cfl, nexec)
+    bounds = [(k * (n // npatch) + min(k, n % npatch), n // npatch + (1 if k < n % npatch else 0))
+              for k in range(npatch)]
+    dx = 1.0 / n
+    for e in range(nexec):
+        ms = 0.0
+        for i in range(n):
+            r, mo, en = U[:, i]
+            ms = max(ms, abs(mo / r) + math.sqrt(G * oracle.L.orc_pressure(G, r, mo, en) / r))
+        dt = 0.4 * dx / ms
+        assert dt == dts[e]
+        new = U.copy()
+        for s0, m in bounds:
+            idx = np.arange(s0 - h, s0 + m + h) % n
+            new[:, s0:s0 + m] = oracle.patch_stage1d(np.ascontiguousarray(U[:, idx]), m, h, dx, dt, G)[:, h:-h]
+        U = new
+    assert np.array_equal(got, U)
