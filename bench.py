@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--adjoint2d-n", type=int, default=2048)
     ap.add_argument("--adjoint2d-steps", type=int, default=4000)
     ap.add_argument("--no-adjoint2d", action="store_true")
+    ap.add_argument("--adjoint2d-horizons", default="500,1000,2000,4000",
+                    help="horizons of the adjoint2d_study extra (FP32 and rounded-IC FP64 gradients vs FP64)")
     ap.add_argument("--extras", default="batched,adjoint1d,sod1d,adjoint2d",
                     help="comma list of extra measurements to run (with extras on)")
     return ap.parse_args()
@@ -496,6 +498,8 @@ def run_ours(args, ws, rank, local):
             out["sod_1d"] = bench_sod1d()
         if "adjoint2d" in ex and not args.no_adjoint2d:
             out["adjoint_2d_kh"] = bench_adjoint2d(args)
+        if "adjoint2d_study" in ex:
+            out["adjoint_2d_study"] = bench_adjoint2d_study(args)
         out["gpu_launches_extras"] = sum(out[k]["launches"] for k in ("batched_kh", "adjoint_1d", "sod_1d")
                                          if k in out)
     if ws == 1 and not args.no_cpu_baseline:
@@ -726,6 +730,87 @@ def bench_adjoint2d(args):
     out.update({"n": n, "steps": K, "policy": "binomial (snapshots fitting 40 GB)",
                 "loss": "integral of 1/2 rho v^2 dA at t_end", "gradient": "d loss / d v(t=0)",
                 "launches": None})
+    return out
+
+
+def kh_grad_v(U0, n, K, prec_np, slots_budget=40e9):
+    """d loss / d v(t=0) of the config-5 loss (integral of 1/2 rho v^2 dA at
+    step K) through the checkpointed adjoint; returns (gradient, dts, stats)."""
+    import nest_b200 as nb
+    from nest_b200.adjoint import BINOMIAL, Adjoint
+    prec = nb.F64 if prec_np == np.float64 else nb.F32
+    s = nb.Solver(2, n, n, bc=nb.BC_PERIODIC, precision=prec)
+    _, pitch, vs = s.state_ptr()
+    slots = int(min(K, slots_budget // (4 * vs * np.dtype(prec_np).itemsize)))
+    s.upload(U0.astype(prec_np))
+    a = Adjoint(s, K, BINOMIAL, slots)
+    a.forward(0.4)
+    L, lam = ke_v(s.download(), n, n)
+    lam0 = a.backward(lam.astype(prec_np)).astype(np.float64)
+    g = lam0[2, 2:-2, 2:-2] * U0[0, 2:-2, 2:-2] + lam0[3, 2:-2, 2:-2] * U0[2, 2:-2, 2:-2]
+    dts, st = a.dts(), a.stats()
+    a.close()
+    s.close()
+    return g, dts, dict(st, loss=L)
+
+
+def bench_adjoint2d_study(args):
+    """Config-5 gradient study (Kelvin-Helmholtz, n x n periodic, seed 1).
+    For each horizon K: the FP32 gradient against the FP64 gradient, and, as
+    a control, the FP64 gradient of the same initial state rounded once
+    through FP32 (a perturbation of about 1e-8 relative) against the FP64
+    gradient.  If the control decorrelates like FP32 does, the disagreement
+    is the flow's sensitivity (chaotic roll-up), not an error of either
+    adjoint.  At the longest horizon the FP64 gradient is also checked by
+    central differences along smooth directions of the initial v field (dts
+    frozen from the FP64 forward sweep)."""
+    import nest_b200 as nb
+    from nest_b200.problems import kelvin_helmholtz
+    n = args.adjoint2d_n
+    hs = [int(x) for x in args.adjoint2d_horizons.split(",")]
+    U0 = kelvin_helmholtz(n, n, seed=1)
+    U0r = U0.astype(np.float32).astype(np.float64)
+
+    def cmp(a, b):
+        return {"rel_l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+                "cosine": float(np.sum(a * b) / (np.linalg.norm(a) * np.linalg.norm(b)))}
+
+    out = {"n": n, "horizons": {}}
+    last = None
+    for K in hs:
+        g64, dts, st64 = kh_grad_v(U0, n, K, np.float64)
+        g64r, _, _ = kh_grad_v(U0r, n, K, np.float64)
+        g32, _, _ = kh_grad_v(U0, n, K, np.float32)
+        out["horizons"][str(K)] = {"f32_vs_f64": cmp(g32, g64), "f64_rounded_ic_vs_f64": cmp(g64r, g64),
+                                   "grad_l2": {"f64": float(np.linalg.norm(g64)), "f64_rounded_ic":
+                                               float(np.linalg.norm(g64r)), "f32": float(np.linalg.norm(g32))}}
+        last = (K, g64, dts, st64["loss"])
+    K, g64, dts, L0 = last
+    x = (np.arange(n) + 0.5) / n
+    fd = []
+    for (m, k, ph) in ((1, 2, 0.1), (2, 1, 0.35), (3, 3, 0.7)):
+        d = np.outer(np.sin(2 * np.pi * (m * x + ph)), np.cos(2 * np.pi * k * x))
+        ad = float(np.sum(g64 * d))
+
+        def L(eps):
+            U = U0[:, 2:-2, 2:-2].copy()
+            r, mv = U[0], U[2]
+            U[3] = U[3] + mv * eps * d + 0.5 * r * (eps * d) ** 2
+            U[2] = mv + r * eps * d
+            s = nb.Solver(2, n, n, bc=nb.BC_PERIODIC, precision=nb.F64)
+            s.freeze_dts(dts)
+            s.upload(U, nb.LAYOUT_INTERIOR)
+            s.step(K, 0.4)
+            val = ke_v(s.download(), n, n)[0]
+            s.close()
+            return val
+        row = {"mode": [m, k], "adjoint": ad}
+        for eps in (1e-4, 1e-6):
+            f = (L(eps) - L(-eps)) / (2 * eps)
+            row[f"fd_eps_{eps:g}"] = f
+            row[f"rel_err_eps_{eps:g}"] = abs(ad - f) / max(abs(f), 1e-300)
+        fd.append(row)
+    out["fd_check_f64"] = {"steps": K, "directions": fd}
     return out
 
 

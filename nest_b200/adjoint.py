@@ -1,12 +1,13 @@
 """Discrete adjoint with checkpointing (nest_adjoint_* in include/nest_b200.h)
 and its torch.autograd.Function.
 
-``Adjoint`` records a forward sweep of a 1D FP64 periodic solver and maps the
-adjoint of the final conserved state to the adjoint of the initial one with
-the same frozen dt sequence.  ``EulerRollout1D`` wraps it as an autograd
-function: U_T = rollout(U_0), so that gradients of any torch loss of U_T
-flow back to U_0 (and, through torch, to whatever produced U_0, e.g. the
-primitive fields)."""
+``Adjoint`` records a forward sweep of a periodic solver (1D FP64 and FP32,
+2D FP64 and FP32) and maps the adjoint of the final conserved state to the
+adjoint of the initial one with the same frozen dt sequence.
+``EulerRollout1D`` / ``EulerRollout2D`` wrap it as autograd functions:
+U_T = rollout(U_0), so that gradients of any torch loss of U_T flow back to
+U_0 (and, through torch, to whatever produced U_0, e.g. the primitive fields
+or an initial perturbation)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -130,8 +131,55 @@ def _autograd_function():
     return EulerRollout1D
 
 
+def _autograd_function_2d():
+    import torch
+
+    class EulerRollout2D(torch.autograd.Function):
+        """U_T = rollout(U_0) for a periodic 2D solver, FP64 (float64 tensor)
+        or the FP32 form (float32 tensor).
+
+        U0: CUDA tensor [4, nx, ny] (interior conserved state rho, rho u,
+        rho v, E; y fastest).  The forward pass records dts (CFL) or uses
+        `dts`; the backward pass runs the checkpointed discrete adjoint of the
+        2D stage (uniform or binomial snapshots) with those dts."""
+
+        @staticmethod
+        def forward(ctx, U0, nsteps: int, cfl: float = 0.4, policy: int = BINOMIAL, param: int = 64,
+                    dts=None, gamma: float = 1.4):
+            _, nx, ny = U0.shape
+            prec = A.F64 if U0.dtype == torch.float64 else A.F32
+            s = Solver(2, nx, ny, bc=A.BC_PERIODIC, gamma=gamma, precision=prec)
+            U0c = U0.detach().contiguous()
+            torch.cuda.current_stream().synchronize()
+            s.upload_device(U0c.data_ptr(), A.LAYOUT_INTERIOR)
+            adj = Adjoint(s, nsteps, policy, param)
+            adj.forward(cfl, dts)
+            UT = torch.empty_like(U0c)
+            s.download_device(UT.data_ptr(), A.LAYOUT_INTERIOR)
+            ctx.adj, ctx.solver, ctx.shape = adj, s, (nx, ny)
+            return UT
+
+        @staticmethod
+        def backward(ctx, gUT):
+            nx, ny = ctx.shape
+            _, pitch, vs = ctx.solver.state_ptr()
+            # adjoint arrays in the solver's device layout: plane k at k * vs,
+            # row i (-2 .. nx+1) at (i + 2) * pitch, column j at j + 2
+            lam = torch.zeros(4 * vs, dtype=gUT.dtype, device=gUT.device)
+            planes = lam.view(4, vs)[:, :(nx + 4) * pitch].view(4, nx + 4, pitch)
+            planes[:, 2:nx + 2, 2:ny + 2] = gUT
+            lam0 = torch.empty_like(lam)
+            torch.cuda.current_stream().synchronize()
+            ctx.adj.backward_device(lam.data_ptr(), lam0.data_ptr())
+            g0 = lam0.view(4, vs)[:, :(nx + 4) * pitch].view(4, nx + 4, pitch)[:, 2:nx + 2, 2:ny + 2]
+            return g0.contiguous(), None, None, None, None, None, None
+
+    return EulerRollout2D
+
+
 class _Lazy:
     fn = None
+    fn2 = None
 
 
 def rollout_1d(U0, nsteps: int, cfl: float = 0.4, policy: int = UNIFORM, param: int = 64, dts=None,
@@ -140,3 +188,11 @@ def rollout_1d(U0, nsteps: int, cfl: float = 0.4, policy: int = UNIFORM, param: 
     if _Lazy.fn is None:
         _Lazy.fn = _autograd_function()
     return _Lazy.fn.apply(U0, nsteps, cfl, policy, param, dts, gamma)
+
+
+def rollout_2d(U0, nsteps: int, cfl: float = 0.4, policy: int = BINOMIAL, param: int = 64, dts=None,
+               gamma: float = 1.4):
+    """Differentiable 2D periodic rollout (torch); see EulerRollout2D."""
+    if _Lazy.fn2 is None:
+        _Lazy.fn2 = _autograd_function_2d()
+    return _Lazy.fn2.apply(U0, nsteps, cfl, policy, param, dts, gamma)

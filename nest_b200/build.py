@@ -29,6 +29,7 @@ UNITS = {
     "euler1d.cu": ["-fmad=false"],
     "euler1d_f32.cu": ["-use_fast_math"],
     "euler2d_f64.cu": ["-fmad=false"],
+    "euler2d_f64r.cu": ["-fmad=false"],
     "euler2d_f32.cu": ["-use_fast_math"],
     "euler2d_f32x2.cu": ["-use_fast_math"],
     "euler2d_compat.cu": ["-fmad=false"],

@@ -264,12 +264,12 @@ nest_status nest_solver_create(const nest_solver_desc* d, nest_solver** out) {
     s->d = *d;
     s->h = d->halo;
     s->esize = d->precision == NEST_F64 ? 8 : 4;
-    // default 2D launch shape: the autotuner's choice at 4096^2 (FP32 16-row
-    // tiles, FP64 32-row tiles, one warp per block).  At 2048^2 the earlier
+    // default 2D launch shape: the autotuner's choice at 4096^2 (16-row
+    // tiles, one warp per block, both precisions).  At 2048^2 the earlier
     // default of 64-row tiles and 4 warps per block left half the warp slots
     // empty: a 4000-step FP32 KH forward took 891 ms against 540 ms.
     if (d->dim == 2) {
-        s->tx = d->precision == NEST_F32 ? 16 : 32;
+        s->tx = 16;
         s->warps = 1;
     }
     if (d->dim == 1) {

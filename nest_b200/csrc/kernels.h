@@ -40,6 +40,11 @@ cudaError_t launch_2d_prepare_f64(double* U, const Geo2D& g, StepCtrl* ctrl, int
 cudaError_t launch_2d_step_f64(double* U, double* U1, const Geo2D& g, const LoopParams& lp,
                                StepCtrl* ctrl, double* partials, int p, int tx, int warps,
                                int which, cudaStream_t st, double* Uout = nullptr);
+// The same FP64 stages as a row march fed by shared-memory rings (bit for bit
+// the same results).
+cudaError_t launch_2d_step_f64r(double* U, double* U1, const Geo2D& g, const LoopParams& lp, StepCtrl* ctrl,
+                                double* partials, int p, int tx, int warps, int which, cudaStream_t st,
+                                double* Uout = nullptr);
 cudaError_t launch_2d_prepare_f32(float* U, const Geo2D& g, StepCtrl* ctrl, int p, cudaStream_t st);
 cudaError_t launch_2d_step_f32(float* U, float* U1, const Geo2D& g, const LoopParams& lp,
                                StepCtrl* ctrl, double* partials, int p, int tx, int warps,

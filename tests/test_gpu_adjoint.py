@@ -340,3 +340,57 @@ def test_adjoint1d_fp32_vs_fp64(gpu):
     g64, g32 = grads[gpu.F64], grads[gpu.F32]
     rel = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
     assert np.all(np.isfinite(g32)) and rel < 1e-3, rel
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_autograd_rollout_2d(gpu, prec):
+    """rollout_2d (torch.autograd.Function over the 2D adjoint): the gradient
+    of a torch loss of U_T w.r.t. the initial v perturbation equals the
+    Adjoint API's bit for bit (same snapshots, same kernels), and in FP64 a
+    finite difference of the loss (dts frozen) to 1e-6."""
+    import torch
+    from nest_b200.adjoint import BINOMIAL, Adjoint, rollout_2d
+    from nest_b200.problems import fourier_fields_2d
+    nx, ny, nsteps = 48, 40, 30
+    tdt = torch.float64 if prec == "f64" else torch.float32
+    U0np = fourier_fields_2d(nx, ny, 4)[:, 2:-2, 2:-2]
+    base = torch.tensor(U0np, dtype=torch.float64, device="cuda")
+    dv = torch.zeros((nx, ny), dtype=torch.float64, device="cuda", requires_grad=True)
+    rho = base[0]
+    U0 = torch.stack([base[0], base[1], base[2] + rho * dv, base[3] + base[2] * dv]).to(tdt)
+    UT = rollout_2d(U0, nsteps, cfl=0.4, policy=BINOMIAL, param=6)
+    v = UT[2].double() / UT[0].double()
+    loss = 0.5 * (UT[0].double() * v * v).sum() / (nx * ny)
+    loss.backward()
+    g = dv.grad.cpu().numpy()
+    assert np.all(np.isfinite(g)) and np.abs(g).max() > 0
+    # the same gradient through the Adjoint API
+    s = gpu.Solver(2, nx, ny, bc=gpu.BC_PERIODIC, precision=gpu.F64 if prec == "f64" else gpu.F32)
+    Uext = np.zeros((4, nx + 4, ny + 4))
+    Uext[:, 2:-2, 2:-2] = U0.detach().double().cpu().numpy()
+    s.upload(Uext.astype(np.float64 if prec == "f64" else np.float32))
+    a = Adjoint(s, nsteps, BINOMIAL, 6)
+    a.forward(0.4)
+    L0, lamT = ke_v_loss_and_lambda(s.download(), nx, ny)
+    lam0 = a.backward(lamT.astype(np.float64 if prec == "f64" else np.float32)).astype(np.float64)
+    want = lam0[2, 2:-2, 2:-2] * U0np[0] + lam0[3, 2:-2, 2:-2] * U0np[2]
+    tol = 1e-10 if prec == "f64" else 1e-5
+    assert np.allclose(g, want, rtol=tol, atol=tol * np.abs(want).max())
+    if prec == "f64":
+        dts = a.dts()
+        x = (np.arange(nx) + 0.5) / nx
+        d = np.outer(np.sin(2 * np.pi * x), np.cos(4 * np.pi * (np.arange(ny) + 0.5) / ny))
+
+        def L(eps):
+            U = U0np.copy()
+            U[3] = U0np[3] + U0np[2] * eps * d + 0.5 * U0np[0] * (eps * d) ** 2
+            U[2] = U0np[2] + U0np[0] * eps * d
+            s2 = gpu.Solver(2, nx, ny, bc=gpu.BC_PERIODIC, precision=gpu.F64)
+            s2.freeze_dts(dts)
+            s2.upload(U, gpu.LAYOUT_INTERIOR)
+            s2.step(nsteps, 0.4)
+            return ke_v_loss_and_lambda(s2.download(), nx, ny)[0]
+
+        fd = (L(1e-7) - L(-1e-7)) / 2e-7
+        ad = float(np.sum(g * d))
+        assert abs(ad - fd) <= 1e-6 * abs(fd), (ad, fd)
