@@ -358,6 +358,7 @@ nest_status nest_solver_load(nest_solver* s, const char* path);
 /* Set the solver clock (time, completed steps). */
 nest_status nest_solver_set_time(nest_solver* s, double time, int steps);
 
+
 #ifdef __cplusplus
 }
 #endif

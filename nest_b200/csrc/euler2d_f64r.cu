@@ -23,6 +23,10 @@
 namespace nestb {
 namespace {
 
+#ifndef NEST_F64R_UNROLL
+#define NEST_F64R_UNROLL 1
+#endif
+constexpr int kUnrollD = NEST_F64R_UNROLL;  // row-loop unroll
 constexpr int LOOKD = 3;                   // stage-input rows in flight ahead of the march
 constexpr int RING_UD = 4, RING_ND = 2;    // ring slots: stage input, U^n (stage 2)
 __host__ __device__ constexpr int ring_d_per_warp(int stage) { return (RING_UD + (stage == 2 ? RING_ND : 0)) * 4 * 32; }
@@ -142,6 +146,7 @@ __device__ __forceinline__ void f64r_body(const StageArgs<double>& a, int strip,
 
     double smx = 0.0, smy = 0.0;
     double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+#pragma unroll kUnrollD
     for (int k = 0; k < rows; ++k) {
         const int i = i0 + k;
         // refill the slots of row i-1 once every lane has read them; then
@@ -230,7 +235,7 @@ __device__ __forceinline__ void f64r_body(const StageArgs<double>& a, int strip,
     }
 }
 
-// Register budget (0: ptxas's choice).
+// Row-loop unroll and register budget (0: ptxas's choice).
 #ifndef NEST_F64R_REGS
 #define NEST_F64R_REGS 0
 #endif
