@@ -170,6 +170,29 @@ nest_status nest_solver_stream(nest_solver* s, void** stream);
 nest_status nest_solver_state_ptr(nest_solver* s, void** dev, long long* pitch, long long* vstride);
 
 /* ------------------------------------------------------------------------ */
+/* Several GPUs: the x-slab step loop in C++ with NCCL.                     */
+/* One rank per GPU holds one x-slab solver (nest_solver_set_exchange_sides */
+/* marks its cut sides).  nest_slab_step enqueues, per step and on the      */
+/* solver's stream: a MAX all-reduce of the two wave-speed words, the two   */
+/* ghost rows of each cut side from the neighbour ranks (NCCL send / recv,  */
+/* one message per variable plane and side), stage 1, the same exchange of  */
+/* the stage buffer, stage 2 (nest's exchange-before-each-stage, examples/  */
+/* sod2d/sod2d.cpp:331-362); runs of 16 steps are replayed from captured    */
+/* CUDA graphs; it returns without waiting.  lo / hi: neighbour ranks, -1   */
+/* for a domain boundary (a rank can be its own neighbour).  NCCL is loaded */
+/* at run time; NEST_ERR_UNSUPPORTED if it is absent.  Destroy solvers (or  */
+/* the communicator) before tearing the process group down: their graphs   */
+/* hold NCCL calls.                                                         */
+/* ------------------------------------------------------------------------ */
+typedef struct nest_slab_comm nest_slab_comm;
+/* Rank 0 makes the communicator id (128 bytes) and sends it to the others. */
+nest_status nest_slab_comm_id(unsigned char id[128]);
+nest_status nest_slab_comm_create(const unsigned char id[128], int nranks, int rank, nest_slab_comm** out);
+nest_status nest_slab_comm_destroy(nest_slab_comm* c);
+nest_status nest_slab_step(nest_solver* s, nest_slab_comm* c, int lo, int hi, int nsteps, double cfl,
+                           double t_final);
+
+/* ------------------------------------------------------------------------ */
 /* Batched independent 2D problems (uneven sizes).  One persistent launch   */
 /* per stage walks a device work list of (problem, column strip, row tile); */
 /* each problem keeps its own dt, time and FP64 totals; runs of steps are   */

@@ -45,6 +45,7 @@ UNITS = {
     "adjoint2d_f64rm.cu": ["-fmad=false"],
     "datio.cpp": ["-x", "cu", "-Xcompiler", "-ffp-contract=off"],
     "pipeline.cu": ["-fmad=false"],
+    "slab.cpp": ["-x", "cu"],
 }
 
 

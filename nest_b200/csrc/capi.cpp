@@ -68,6 +68,7 @@ namespace {
 nest_status drop_graphs(nest_solver* s) {
     for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second);
     s->graphs.clear();
+    slab_release(s);
     return NEST_OK;
 }
 

@@ -96,5 +96,7 @@ nest_status prepare(nest_solver* s);
 // Enqueue one step (which: 1 = stage 1, 2 = stage 2, 3 = both) on the solver's buffers.
 cudaError_t enqueue_step(nest_solver* s, const LoopParams& lp, int p, int which = 3);
 nest_status read_ctrl(nest_solver* s);
+// Releases the slab driver's captured step graphs of a solver (slab.cpp).
+void slab_release(nest_solver* s);
 }  // namespace rt
 }  // namespace nestb

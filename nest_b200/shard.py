@@ -208,14 +208,71 @@ class SlabDomain:
                     s.stage(2, cfl, t_final)
 
 
+def native_peers(k: int, nslabs: int, periodic: bool) -> tuple[int, int]:
+    """Neighbour ranks (lo, hi) of slab k for the native driver, -1 at a
+    domain boundary; a periodic one-slab domain is its own neighbour."""
+    if periodic:
+        return (k - 1) % nslabs, (k + 1) % nslabs
+    return (k - 1 if k > 0 else -1), (k + 1 if k < nslabs - 1 else -1)
+
+
+class NativeSlabDomain:
+    """This rank's x-slab stepped by the C++ driver (nest_slab_step): the
+    speed all-reduce and the ghost-row exchanges go through NCCL on the
+    solver's stream and runs of 16 steps replay from CUDA graphs, so no
+    Python runs per step.  Same interface as SlabDomain for one slab."""
+
+    def __init__(self, slab: GPUSlab, k: int, nslabs: int, periodic: bool, group=None):
+        import ctypes as C
+        import torch
+        from ._capi import check, lib
+        A.bind({
+            "nest_slab_comm_id": (C.c_int, [C.c_char_p]),
+            "nest_slab_comm_create": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+            "nest_slab_comm_destroy": (C.c_int, [C.c_void_p]),
+            "nest_slab_step": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double]),
+        })
+        self.slabs, self.ids, self.nslabs = [slab], [k], nslabs
+        idbuf = C.create_string_buffer(128)
+        if group is None or k == 0:
+            check(lib.nest_slab_comm_id(idbuf), "nest_slab_comm_id")
+        if group is not None:
+            import torch.distributed as dist
+            obj = [bytes(idbuf.raw)]
+            dist.broadcast_object_list(obj, src=dist.get_global_rank(group, 0) if group is not dist.group.WORLD else 0,
+                                       group=group)
+            idbuf = C.create_string_buffer(obj[0], 128)
+        h = C.c_void_p()
+        torch.cuda.synchronize()
+        check(lib.nest_slab_comm_create(idbuf, nslabs, k, C.byref(h)), "nest_slab_comm_create")
+        self._comm = h
+        self.lo, self.hi = native_peers(k, nslabs, periodic)
+        self._lib, self._check = lib, check
+
+    def step(self, nsteps: int, cfl: float, t_final: float = 0.0):
+        self._check(self._lib.nest_slab_step(self.slabs[0].solver._h, self._comm, self.lo, self.hi, nsteps, cfl,
+                                             t_final), "nest_slab_step")
+
+    def close(self):
+        """Release the solvers' graphs, then the communicator."""
+        if getattr(self, "_comm", None):
+            for s in self.slabs:
+                s.solver.close()
+            self._lib.nest_slab_comm_destroy(self._comm)
+            self._comm = None
+
+
 def gpu_domain(nx: int, ny: int, *, bc: int = A.BC_PERIODIC, precision: int = A.F64, gamma: float = 1.4,
-               flags: int = 0, group=None, local_slabs: int = 1):
+               flags: int = 0, group=None, local_slabs: int = 1, native: bool = False, nslabs: int | None = None):
     """Slabs of an nx x ny domain on [0,1]^2 for this process.
 
     With a torch.distributed group of W ranks, rank r holds slab r of W
     (one per device, the caller sets the current device); without one the
     process holds `local_slabs` slabs on the current device, sharing one
-    stream.  Returns (SlabDomain, [(x0, n) per held slab])."""
+    stream.  native=True: this process's single slab is stepped by the C++
+    NCCL driver (NativeSlabDomain); without a group that is a one-rank
+    domain whose periodic neighbour is itself.  Returns (domain,
+    [(x0, n) per held slab])."""
     import torch
     if group is not None:
         import torch.distributed as dist
@@ -229,10 +286,18 @@ def gpu_domain(nx: int, ny: int, *, bc: int = A.BC_PERIODIC, precision: int = A.
     slabs, ranges = [], []
     for k in ids:
         x0, n = slab_range(nx, W, k)
-        lo_ex = W > 1 and (periodic or k > 0)
-        hi_ex = W > 1 and (periodic or k < W - 1)
+        if native:  # exchange sides are the sides with a neighbour rank
+            lo, hi = native_peers(k, W, periodic)
+            lo_ex, hi_ex = lo >= 0, hi >= 0
+        else:
+            lo_ex = W > 1 and (periodic or k > 0)
+            hi_ex = W > 1 and (periodic or k < W - 1)
         slabs.append(GPUSlab(n, ny, 1.0 / nx, 1.0 / ny, bc, precision, lo_ex, hi_ex, gamma, flags, stream))
         ranges.append((x0, n))
+    if native:
+        if len(slabs) != 1:
+            raise ValueError("the native driver steps one slab per process")
+        return NativeSlabDomain(slabs[0], ids[0], W, periodic, group), ranges
     return SlabDomain(slabs, ids, W, periodic, group, owner), ranges
 
 

@@ -63,3 +63,27 @@ def test_exchange_sides_checks(gpu):
     s2 = gpu.Solver(2, 32, 32, flags=gpu.FLAG_SPLIT_COMPAT)
     with pytest.raises(gpu.NestError):
         s2.set_exchange_sides(True, False)
+
+
+@pytest.mark.parametrize("prec", ["F64", "F32"])
+@pytest.mark.parametrize("bc,nx,ny,nsteps", [(0, 130, 96, 37), (1, 96, 80, 20)])
+def test_native_driver_one_rank_equals_one_domain(gpu, prec, bc, nx, ny, nsteps):
+    """The C++ slab driver (nest_slab_step: NCCL speed all-reduce and
+    ghost-row send / recv on the solver's stream, 16-step CUDA graphs) on a
+    one-rank domain: periodic x exchanges the slab's rows with itself through
+    NCCL, outflow has no cut side.  The result equals the one-domain solver
+    bit for bit (37 steps: two graph replays and five single steps)."""
+    import torch
+    from nest_b200.shard import gpu_domain, slab_rows
+    prec = getattr(gpu, prec)
+    U = kelvin_helmholtz(nx, ny, seed=5) if bc == gpu.BC_PERIODIC else riemann_2d(nx, ny)
+    dom, ranges = gpu_domain(nx, ny, bc=bc, precision=prec, native=True)
+    (slab,), ((x0, n),) = dom.slabs, ranges
+    slab.solver.upload(slab_rows(U, x0, n).astype(np.float64 if prec == gpu.F64 else np.float32))
+    dom.step(nsteps, 0.4)
+    torch.cuda.synchronize()
+    got, t = slab.solver.download()[:, 2:-2, 2:-2], slab.solver.time()
+    want, t1 = run_one(gpu, U, nx, ny, bc, prec, nsteps)
+    dom.close()
+    assert np.array_equal(got, want)
+    assert t == t1

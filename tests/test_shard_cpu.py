@@ -150,3 +150,14 @@ def test_gloo_ranks_equal_one_domain(oracle, tmp_path, bc, world):
     got = np.concatenate([np.load(tmp_path / f"slab{r}.npy") for r in range(world)], axis=1)
     U = kelvin_helmholtz(nx, ny, seed=9) if bc == 0 else riemann_2d(nx, ny)
     assert np.array_equal(got, one_domain(oracle, U, nx, ny, bc, nsteps))
+
+
+def test_native_driver_neighbours():
+    """Neighbour ranks of the native slab driver: periodic rings (a one-slab
+    domain is its own neighbour on both sides), open chains end in -1."""
+    from nest_b200.shard import native_peers
+    assert native_peers(0, 1, True) == (0, 0)
+    assert native_peers(0, 1, False) == (-1, -1)
+    assert [native_peers(k, 3, True) for k in range(3)] == [(2, 1), (0, 2), (1, 0)]
+    assert [native_peers(k, 3, False) for k in range(3)] == [(-1, 1), (0, 2), (1, -1)]
+    assert native_peers(0, 2, True) == (1, 1) and native_peers(1, 2, True) == (0, 0)
