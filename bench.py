@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the batched-KH and adjoint measurements")
     ap.add_argument("--slab-path", action="store_true",
                     help="drive the domain through the x-slab driver even on one GPU (a one-rank group)")
+    ap.add_argument("--native-slabs", action="store_true",
+                    help="x-slabs stepped by the C++ NCCL driver (nest_slab_step, graph-replayed) instead of "
+                         "the per-step torch.distributed loop")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=500)
     ap.add_argument("--adjoint-n", type=int, default=65536)
@@ -291,7 +294,8 @@ def run_slabs(args, ws, rank, form, cfl, st):
     from nest_b200.tuning import best_tiling
     n = args.n
     prec, flags = form_args(form)
-    dom, ranges = gpu_domain(ws * n, n, bc=nb.BC_OUTFLOW, precision=prec, flags=flags, group=dist.group.WORLD)
+    dom, ranges = gpu_domain(ws * n, n, bc=nb.BC_OUTFLOW, precision=prec, flags=flags, group=dist.group.WORLD,
+                             native=args.native_slabs)
     (slab,), ((x0, nl),) = dom.slabs, ranges
     U = riemann_2d(ws * n, n, rows=(x0, nl))
     U = U.astype(np.float32) if prec == nb.F32 else U
@@ -318,21 +322,25 @@ def run_slabs(args, ws, rank, form, cfl, st):
     # per-kernel durations: the same steps again with events around each stage
     slab.solver.upload(U)
     slab.solver.reset_time()
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-    with slab.stream():
-        for k in range(args.steps):
-            dom.reduce_speeds()
-            dom.exchange(0)
-            ev[k][0].record(sst)
-            slab.stage(1, cfl, 0.0)
-            ev[k][1].record(sst)
-            dom.exchange(1)
-            ev[k][2].record(sst)
-            slab.stage(2, cfl, 0.0)
-            ev[k][3].record(sst)
-    sst.synchronize()
-    k1 = [e[0].elapsed_time(e[1]) for e in ev]
-    k2 = [e[2].elapsed_time(e[3]) for e in ev]
+    if args.native_slabs:
+        # the stage kernels alone (their durations do not depend on the exchanges)
+        k1, k2, _ = slab.solver.step_profiled(args.steps, cfl)
+    else:
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+        with slab.stream():
+            for k in range(args.steps):
+                dom.reduce_speeds()
+                dom.exchange(0)
+                ev[k][0].record(sst)
+                slab.stage(1, cfl, 0.0)
+                ev[k][1].record(sst)
+                dom.exchange(1)
+                ev[k][2].record(sst)
+                slab.stage(2, cfl, 0.0)
+                ev[k][3].record(sst)
+        sst.synchronize()
+        k1 = [e[0].elapsed_time(e[1]) for e in ev]
+        k2 = [e[2].elapsed_time(e[3]) for e in ev]
     out = {"ms": ms, "k1": k1, "k2": k2, "tsim": tsim, "steps": nst, "tiling": tiling, "window": (t0, t1),
            "cells_local": nl * n, "graph_ms": None}
     if not args.no_e2e:
@@ -357,8 +365,11 @@ def run_slabs(args, ws, rank, form, cfl, st):
                       "api": "nest_solver_upload -> SlabDomain.step -> nest_solver_download -> nest_solver_time"}
     barrier(ws)
     torch.cuda.synchronize()
-    for sl in dom.slabs:
-        sl.solver.close()
+    if args.native_slabs:
+        dom.close()  # graphs holding NCCL calls go before the communicator
+    else:
+        for sl in dom.slabs:
+            sl.solver.close()
     return out
 
 
@@ -735,7 +746,8 @@ def bench_adjoint2d(args):
 
 def kh_grad_v(U0, n, K, prec_np, slots_budget=40e9):
     """d loss / d v(t=0) of the config-5 loss (integral of 1/2 rho v^2 dA at
-    step K) through the checkpointed adjoint; returns (gradient, dts, stats)."""
+    step K) through the checkpointed adjoint; returns (gradient, dts, stats
+    with the loss and the final density)."""
     import nest_b200 as nb
     from nest_b200.adjoint import BINOMIAL, Adjoint
     prec = nb.F64 if prec_np == np.float64 else nb.F32
@@ -745,31 +757,38 @@ def kh_grad_v(U0, n, K, prec_np, slots_budget=40e9):
     s.upload(U0.astype(prec_np))
     a = Adjoint(s, K, BINOMIAL, slots)
     a.forward(0.4)
-    L, lam = ke_v(s.download(), n, n)
+    UT = s.download()
+    L, lam = ke_v(UT, n, n)
     lam0 = a.backward(lam.astype(prec_np)).astype(np.float64)
     g = lam0[2, 2:-2, 2:-2] * U0[0, 2:-2, 2:-2] + lam0[3, 2:-2, 2:-2] * U0[2, 2:-2, 2:-2]
     dts, st = a.dts(), a.stats()
     a.close()
     s.close()
-    return g, dts, dict(st, loss=L)
+    return g, dts, dict(st, loss=L, rho=UT[0, 2:-2, 2:-2].astype(np.float64))
 
 
 def bench_adjoint2d_study(args):
     """Config-5 gradient study (Kelvin-Helmholtz, n x n periodic, seed 1).
     For each horizon K: the FP32 gradient against the FP64 gradient, and, as
-    a control, the FP64 gradient of the same initial state rounded once
-    through FP32 (a perturbation of about 1e-8 relative) against the FP64
-    gradient.  If the control decorrelates like FP32 does, the disagreement
-    is the flow's sensitivity (chaotic roll-up), not an error of either
-    adjoint.  At the longest horizon the FP64 gradient is also checked by
-    central differences along smooth directions of the initial v field (dts
-    frozen from the FP64 forward sweep)."""
+    controls, FP64 gradients of perturbed initial states against the FP64
+    gradient: the state rounded once through FP32 (about 1e-8 relative) and
+    seeded relative noise of 1e-6 and 1e-5 on every conserved field.  Each
+    run also reports how far its final density lies from the FP64 run's
+    (relative L2), so the FP32 trajectory's deviation can be set beside the
+    controls'.  If a control whose trajectory deviates as much as FP32's
+    decorrelates like FP32 does, the disagreement is the flow's sensitivity,
+    not an error of either adjoint.  At the longest horizon the FP64 gradient
+    is also checked by central differences along smooth directions of the
+    initial v field (dts frozen from the FP64 forward sweep)."""
     import nest_b200 as nb
     from nest_b200.problems import kelvin_helmholtz
     n = args.adjoint2d_n
     hs = [int(x) for x in args.adjoint2d_horizons.split(",")]
     U0 = kelvin_helmholtz(n, n, seed=1)
-    U0r = U0.astype(np.float32).astype(np.float64)
+    rng = np.random.default_rng(11)
+    noise = rng.standard_normal(U0.shape)
+    controls = {"f64_rounded_ic": U0.astype(np.float32).astype(np.float64),
+                "f64_noise_1e-6": U0 * (1 + 1e-6 * noise), "f64_noise_1e-5": U0 * (1 + 1e-5 * noise)}
 
     def cmp(a, b):
         return {"rel_l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
@@ -779,11 +798,15 @@ def bench_adjoint2d_study(args):
     last = None
     for K in hs:
         g64, dts, st64 = kh_grad_v(U0, n, K, np.float64)
-        g64r, _, _ = kh_grad_v(U0r, n, K, np.float64)
-        g32, _, _ = kh_grad_v(U0, n, K, np.float32)
-        out["horizons"][str(K)] = {"f32_vs_f64": cmp(g32, g64), "f64_rounded_ic_vs_f64": cmp(g64r, g64),
-                                   "grad_l2": {"f64": float(np.linalg.norm(g64)), "f64_rounded_ic":
-                                               float(np.linalg.norm(g64r)), "f32": float(np.linalg.norm(g32))}}
+        runs = {"f32": kh_grad_v(U0, n, K, np.float32)}
+        for name, Uc in controls.items():
+            runs[name] = kh_grad_v(Uc, n, K, np.float64)
+        h = {"grad_l2": {"f64": float(np.linalg.norm(g64))}}
+        for name, (g, _, st) in runs.items():
+            h[name + "_vs_f64"] = dict(cmp(g, g64), final_rho_rel_l2=float(
+                np.linalg.norm(st["rho"] - st64["rho"]) / np.linalg.norm(st64["rho"])))
+            h["grad_l2"][name] = float(np.linalg.norm(g))
+        out["horizons"][str(K)] = h
         last = (K, g64, dts, st64["loss"])
     K, g64, dts, L0 = last
     x = (np.arange(n) + 0.5) / n
