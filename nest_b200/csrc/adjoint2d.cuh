@@ -89,12 +89,18 @@ __device__ __forceinline__ void hlle4_adj(T gamma, T igm1, Adj4<T> L, Adj4<T> R,
     side(R, ER, cR, fRb, uRb, nRb, cRb, wr);
 }
 
+// Minmod slope and its branch: 0 none, 1 first difference, 2 second; for
+// FP32 states 3 = a near-tie (|d1| and |d2| within 2^-19 |w| of each other,
+// w the cell's primitive), whose slope adjoint is split half and half between
+// the two differences (the reasoning is at tie_mask in adjoint2d_f32x2.cu).
+// FP64 keeps the exact branch.
 template <typename T>
-__device__ __forceinline__ T mmslope(T d1, T d2, signed char& br) {
+__device__ __forceinline__ T mmslope(T d1, T d2, signed char& br, T w) {
     if (d1 * d2 <= T(0)) { br = 0; return T(0); }
-    if (fabs(d1) < fabs(d2)) { br = 1; return d1; }
-    br = 2;
-    return d2;
+    const bool first = fabs(d1) < fabs(d2);
+    if (sizeof(T) == 4 && fabs(fabs(d1) - fabs(d2)) <= T(1.9073486e-06) * fabs(w)) br = 3;
+    else br = first ? 1 : 2;
+    return first ? d1 : d2;
 }
 
 // Shared-memory image of one tile.
@@ -187,7 +193,8 @@ __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lo
         int a = t / ATY, b = t % ATY;
         for (int k = 0; k < 4; ++k) {
             signed char br;
-            Sx[k][a][b] = mmslope(W[k][a + 1][b + 3] - W[k][a][b + 3], W[k][a + 2][b + 3] - W[k][a + 1][b + 3], br);
+            Sx[k][a][b] = mmslope(W[k][a + 1][b + 3] - W[k][a][b + 3], W[k][a + 2][b + 3] - W[k][a + 1][b + 3], br,
+                                  W[k][a + 1][b + 3]);
             Bx[k][a][b] = br;
         }
     }
@@ -196,7 +203,8 @@ __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lo
         int a = t / RY2, c = t % RY2;
         for (int k = 0; k < 4; ++k) {
             signed char br;
-            Sy[k][a][c] = mmslope(W[k][a + 3][c + 1] - W[k][a + 3][c], W[k][a + 3][c + 2] - W[k][a + 3][c + 1], br);
+            Sy[k][a][c] = mmslope(W[k][a + 3][c + 1] - W[k][a + 3][c], W[k][a + 3][c + 2] - W[k][a + 3][c + 1], br,
+                                  W[k][a + 3][c + 1]);
             By[k][a][c] = br;
         }
     }
@@ -246,12 +254,12 @@ __device__ void adjoint2d_tile(const T* __restrict__ U, const T* __restrict__ Lo
         T v = XR[k][q - 1][b] + XL[k][q][b] + YR[k][a][r - 1] + YL[k][a][r];
         int bx0 = Bx[k][q][b], bxm = Bx[k][q - 1][b], bxp = Bx[k][q + 1][b];
         if (bx0 == 1) v += sbx(k, q); else if (bx0 == 2) v -= sbx(k, q);
-        if (bxm == 2) v += sbx(k, q - 1);
-        if (bxp == 1) v -= sbx(k, q + 1);
+        if (bxm == 2) v += sbx(k, q - 1); else if (bxm == 3) v += T(0.5) * sbx(k, q - 1);
+        if (bxp == 1) v -= sbx(k, q + 1); else if (bxp == 3) v -= T(0.5) * sbx(k, q + 1);
         int by0 = By[k][a][r], bym = By[k][a][r - 1], byp = By[k][a][r + 1];
         if (by0 == 1) v += sby(k, r); else if (by0 == 2) v -= sby(k, r);
-        if (bym == 2) v += sby(k, r - 1);
-        if (byp == 1) v -= sby(k, r + 1);
+        if (bym == 2) v += sby(k, r - 1); else if (bym == 3) v += T(0.5) * sby(k, r - 1);
+        if (byp == 1) v -= sby(k, r + 1); else if (byp == 3) v -= T(0.5) * sby(k, r + 1);
         wb[k] = v;
     }
     const long long o = g.at(i, j);
