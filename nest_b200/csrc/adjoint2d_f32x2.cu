@@ -92,15 +92,18 @@ __device__ __forceinline__ float max3f(float a, float b, float c) {
 // 0.08) while finite differences of the FP32 forward map agreed with the FP64
 // map's to 1e-4; with the split it is 0.011 (cosine 0.99994) and its
 // directional derivatives match those finite differences to about 1 %.
-__device__ __forceinline__ float tie_mask(float s, float d1, float d2, float w) {
-    const float tol = 1.9073486e-06f * fabsf(w);  // 2^-19 |w|
-    if (s != 0.f && fabsf(fabsf(d1) - fabsf(d2)) <= tol) return 0.5f;
-    return s == d2 ? 1.f : 0.f;
+// Where the slope is not zero d1 and d2 have one sign, so ||d1| - |d2|| is
+// |d1 - d2|: one packed subtraction and one packed product per pair.  Where
+// it is zero the mask is not used.
+__device__ __forceinline__ float tie_mask(float s, float d2, float dd, float tol) {
+    // (where the slope is zero the mask is not used: mz = 0)
+    return fabsf(dd) <= fabsf(tol) ? 0.5f : (s == d2 ? 1.f : 0.f);
 }
 __device__ __forceinline__ F2 mm_mask(F2 d1, F2 d2, F2& mz, F2& me, F2 w) {
     F2 s = make_float2(mm(d1.x, d2.x), mm(d1.y, d2.y));
+    const F2 dd = sub2(d1, d2), tol = mul2(sp(1.9073486e-06f), w);  // 2^-19 w
     mz = make_float2(s.x != 0.f ? 1.f : 0.f, s.y != 0.f ? 1.f : 0.f);
-    me = make_float2(tie_mask(s.x, d1.x, d2.x, w.x), tie_mask(s.y, d1.y, d2.y, w.y));
+    me = make_float2(tie_mask(s.x, d2.x, dd.x, tol.x), tie_mask(s.y, d2.y, dd.y, tol.y));
     return s;
 }
 
