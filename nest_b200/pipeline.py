@@ -70,6 +70,9 @@ class Pipeline:
         return self
 
     def execute(self, ptr: int, stream: int | None = None):
+        """All stages once on `stream` (default: the pipeline's own
+        non-blocking stream).  Returns when they are enqueued: read the state
+        after clock() (which waits) or a synchronize of that stream."""
         check(lib.nest_pipeline_execute(self._h, C.c_void_p(ptr), C.c_void_p(stream) if stream else None),
               "nest_pipeline_execute")
 

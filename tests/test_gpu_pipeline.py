@@ -125,10 +125,13 @@ def test_sod1d_example_on_device(gpu, oracle):
     pipe.set_clock()
     d1 = device(pipe.scatter(U0))
     assert pipe.run(d1.data_ptr(), 1e9, max_steps=48) == 48
+    c1 = pipe.clock()
     pipe.set_clock()
     d2 = device(pipe.scatter(U0))
     for _ in range(48):
         pipe.execute(d2.data_ptr())
+    # execute() only enqueues on the pipeline's stream; clock() waits for it
+    assert pipe.clock() == c1
     assert np.array_equal(d1.cpu().numpy(), d2.cpu().numpy())
     pipe.close()
 
