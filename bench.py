@@ -649,7 +649,7 @@ def bench_adjoint(args):
     return {"n": n, "steps": K, "checkpoint_every": 64, "forward_ms": fwd, "backward_ms": bwd, "fd_check": fd,
             "adjoint_over_forward": bwd / fwd, "gradient_over_forward": (fwd + bwd) / fwd,
             "recomputed_steps": st["recomputed_steps"], "checkpoint_mb": st["checkpoint_bytes"] / 1e6,
-            "launches": 2 * (2 * K + 2 * K + 3 * K), "dtype": "f64", "f32": f32}
+            "launches": 2 * (K + 2 * K), "dtype": "f64", "f32": f32}
 
 
 def bench_sod1d(reps: int = 20):

@@ -46,7 +46,8 @@ namespace {
 // pointer.
 struct Stepper {
     virtual ~Stepper() = default;
-    // which = 1: U1 <- S(Un); which = 2: Uout <- (Un + S(U1)) / 2 after stage 1
+    // which = 1: U1 <- S(Un); which = 2: Uout <- (Un + S(U1)) / 2 after stage 1;
+    // which = 3: both (Uout distinct from Un)
     virtual cudaError_t stage(int which, void* Un, void* U1, void* Uout, const LoopParams& lp, int p) = 0;
     virtual cudaError_t adjoint_step(void* Un, void* U1, const double* dtp, void* lam, void* lam_new, void* tmp) = 0;
 };
@@ -63,6 +64,13 @@ struct Stepper1D : Stepper {
     StepCtrl* ctrl;
     explicit Stepper1D(nest_solver* s_, StepCtrl* c) : s(s_), ctrl(c) {}
     cudaError_t stage(int which, void* Un, void* U1, void* Uout, const LoopParams& lp, int p) override {
+        if (which == 3 && Uout && Uout != Un) {  // one launch, U1 of the step kept in U1
+            if (s->d.precision == NEST_F32)
+                return launch_1d_fused_f32((const float*)Un, (float*)Uout, (float*)U1, s->d.nx, s->h, s->d.dx,
+                                           s->d.gamma, s->d.bc_x, lp, ctrl, p, s->st);
+            return launch_1d_fused((const double*)Un, (double*)Uout, (double*)U1, s->d.nx, s->h, s->d.dx,
+                                   s->d.gamma, s->d.bc_x, lp, ctrl, p, s->st);
+        }
         if (s->d.precision == NEST_F32)
             return launch_1d_step_f32((float*)Un, (float*)U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp, ctrl,
                                       p, which, s->st, (float*)Uout);
@@ -242,8 +250,8 @@ nest_status segment_graph(nest_adjoint* a, int L, cudaGraphExec_t* out) {
     lp.dts_in = a->seg_dts;
     lp.dts_cap = L;
     for (int r = 0; r < L && e == cudaSuccess; ++r) {
-        e = a->stepper->stage(1, a->seg_un[r], a->seg_u1[r], nullptr, lp, r & 1);
-        if (e == cudaSuccess && r + 1 < L) e = a->stepper->stage(2, a->seg_un[r], a->seg_u1[r], a->seg_un[r + 1], lp, r & 1);
+        if (r + 1 < L) e = a->stepper->stage(3, a->seg_un[r], a->seg_u1[r], a->seg_un[r + 1], lp, r & 1);
+        else e = a->stepper->stage(1, a->seg_un[r], a->seg_u1[r], nullptr, lp, r & 1);
     }
     int cur = 0;
     for (int r = L - 1; r >= 0 && e == cudaSuccess; --r, cur ^= 1)

@@ -30,7 +30,7 @@
 namespace nestb {
 namespace {
 
-constexpr int TA = 128;       // cells per CTA
+constexpr int TA = 112;       // cells per CTA (586 CTAs at 65536 cells: at most 4 per SM, 448 cells)
 constexpr int NTA = TA + 10;  // threads per CTA: one per cell of the widest phase (TA + 4 outputs + 6)
 
 template <typename T>
@@ -214,6 +214,8 @@ k1d_adjoint_step(const T* __restrict__ Un, const T* __restrict__ U1, const T* __
                  T* __restrict__ lam_new, int n, int h, const double* dtp, double dx, double gamma_d) {
     __shared__ Rev1<T, TA + 4> R;
     __shared__ T tmp[3][TA + 4];  // cells c0-2 .. c0+TA+1
+    pdl_wait();
+    pdl_trigger();
     const T lambda = (T)(*dtp / dx);
     const T gamma = (T)gamma_d, gm1 = (T)(gamma_d - 1.0);
     const int nt = n + 2 * h, c0 = blockIdx.x * TA;
@@ -244,8 +246,7 @@ template <typename T>
 cudaError_t launch_1d_adjoint_step_t(const T* Un, const T* U1, const T* lam, T* lam_new, int n, int h,
                                      const double* dtp, double dx, double gamma, cudaStream_t st) {
     int blocks = (n + TA - 1) / TA;
-    k1d_adjoint_step<T><<<blocks, NTA, 0, st>>>(Un, U1, lam, lam_new, n, h, dtp, dx, gamma);
-    return cudaGetLastError();
+    return launch_pdl(k1d_adjoint_step<T>, dim3(blocks), dim3(NTA), 0, st, Un, U1, lam, lam_new, n, h, dtp, dx, gamma);
 }
 
 }  // namespace

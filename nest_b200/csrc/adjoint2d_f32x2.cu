@@ -87,7 +87,7 @@ __device__ __forceinline__ float max3f(float a, float b, float c) {
 // half between the two differences (the mean of the two one-sided
 // derivatives).  Taking either one instead sent an O(1) share of the slope
 // adjoint to a neighbour chosen by rounding in many cells of a rolled-up
-// Kelvin-Helmholtz layer: after 4000 steps of the 2048^2 config-5 problem the
+// Kelvin-Helmholtz layer: after 4000 steps of the 2048^2 periodic KH problem the
 // FP32 gradient had a relative L2 distance 12.8 from the FP64 one (cosine
 // 0.08) while finite differences of the FP32 forward map agreed with the FP64
 // map's to 1e-4; with the split it is 0.011 (cosine 0.99994) and its

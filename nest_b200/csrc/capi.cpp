@@ -85,7 +85,8 @@ LoopParams base_params(const nest_solver* s) {
 
 // Ghost fill + wave-speed maxima of the current state into slot `parity`.
 nest_status nestb::rt::prepare(nest_solver* s) {
-    CK(cudaMemsetAsync(&s->ctrl->maxs[s->parity][0], 0, 2 * sizeof(unsigned long long), s->st));
+    // both slots: the one-launch 1D step adds into maxs[1 - parity][1]
+    CK(cudaMemsetAsync(&s->ctrl->maxs[0][0], 0, sizeof s->ctrl->maxs, s->st));
     cudaError_t e;
     if (s->d.dim == 1 && s->d.precision == NEST_F32) {
         e = launch_1d_prepare_f32((float*)s->U, s->d.nx, s->h, s->d.gamma, s->d.bc_x, s->ctrl, s->parity, s->st);
@@ -123,13 +124,32 @@ cudaError_t nestb::rt::enqueue_step(nest_solver* s, const LoopParams& lp, int p,
 
 namespace {
 
-// Enqueue nsteps steps of the tiled path; whole chunks go through cached graphs.
+// Two 1D steps with parity p, one launch each, out of place: U -> U1 -> U
+// (the stage buffer holds the state between them, so the state ends where it
+// started).
+cudaError_t enqueue_pair_1d(nest_solver* s, const LoopParams& lp, int p) {
+    auto one = [&](void* from, void* to, int pp) {
+        if (s->d.precision == NEST_F32)
+            return launch_1d_fused_f32((const float*)from, (float*)to, nullptr, s->d.nx, s->h, s->d.dx, s->d.gamma,
+                                       s->d.bc_x, lp, s->ctrl, pp, s->st);
+        return launch_1d_fused((const double*)from, (double*)to, nullptr, s->d.nx, s->h, s->d.dx, s->d.gamma,
+                               s->d.bc_x, lp, s->ctrl, pp, s->st);
+    };
+    cudaError_t e = one(s->U, s->U1, p);
+    if (e == cudaSuccess) e = one(s->U1, s->U, p ^ 1);
+    return e;
+}
+
+// Enqueue nsteps steps of the tiled path; whole chunks go through cached
+// graphs.  1D steps go in pairs of one-launch steps; an odd last step runs
+// the two stage launches in place.
 nest_status enqueue_steps(nest_solver* s, int nsteps, const LoopParams& lp) {
     if (!s->prepared) {
         nest_status r = prepare(s);
         if (r != NEST_OK) return r;
     }
     bool use_graphs = s->st != nullptr;
+    const bool pairs = s->d.dim == 1;
     while (nsteps > 0) {
         if (use_graphs && nsteps >= GRAPH_STEPS) {
             GraphKey k{GRAPH_STEPS, s->parity, lp.cfl, lp.t_final, lp.fixed_dt, lp.max_steps, lp.dts_in,
@@ -140,7 +160,10 @@ nest_status enqueue_steps(nest_solver* s, int nsteps, const LoopParams& lp) {
                 CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
                 int p = s->parity;
                 cudaError_t e = cudaSuccess;
-                for (int i = 0; i < GRAPH_STEPS && e == cudaSuccess; ++i, p ^= 1) e = enqueue_step(s, lp, p);
+                if (pairs)
+                    for (int i = 0; i < GRAPH_STEPS && e == cudaSuccess; i += 2) e = enqueue_pair_1d(s, lp, p);
+                else
+                    for (int i = 0; i < GRAPH_STEPS && e == cudaSuccess; ++i, p ^= 1) e = enqueue_step(s, lp, p);
                 cudaError_t e2 = cudaStreamEndCapture(s->st, &g);
                 if (e != cudaSuccess) return cuda_fail(e, "step capture");
                 if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
@@ -152,6 +175,10 @@ nest_status enqueue_steps(nest_solver* s, int nsteps, const LoopParams& lp) {
             }
             CK(cudaGraphLaunch(it->second, s->st));
             nsteps -= GRAPH_STEPS;  // parity unchanged (even chunk)
+        } else if (pairs && nsteps >= 2) {
+            cudaError_t e = enqueue_pair_1d(s, lp, s->parity);
+            if (e != cudaSuccess) return cuda_fail(e, "step launch");
+            nsteps -= 2;  // parity unchanged
         } else {
             cudaError_t e = enqueue_step(s, lp, s->parity);
             if (e != cudaSuccess) return cuda_fail(e, "step launch");

@@ -15,7 +15,34 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 namespace nestb {
+
+// Programmatic dependent launch (sm_90 and later).  A kernel launched by
+// launch_pdl may be scheduled while the kernel before it in the stream is
+// still running: pdl_wait() returns once that kernel has completed and its
+// memory is visible (immediately for an ordinary launch), so nothing is read
+// before it; pdl_trigger() then lets the next such kernel be scheduled,
+// which hides its launch and block start-up behind this kernel's run.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 // Boundary conditions on the domain edges.
 enum { BC_PERIODIC = 0, BC_OUTFLOW = 1 };
@@ -45,6 +72,11 @@ struct StepCtrl {
     int bad_i, bad_j;               // its interior index (1D: bad_j = 0)
     int pad_;
     double bad_rho, bad_p;          // and its density and pressure
+    // one-launch 1D steps: blocks of the running step that have added their
+    // wave speed to maxs[q][1] (the last one moves the maximum to maxs[q][0],
+    // clears maxs[q][1] and resets this count)
+    unsigned blocks_done;
+    unsigned pad2_;
 };
 
 // Time-loop parameters shared by all launches of a solver.
@@ -131,7 +163,10 @@ __device__ __forceinline__ double prescribed_dt(const StepCtrl* c, int p, const 
 }
 
 // Block 0 / thread 0 of stage 1: publish dt and prepare the next slot.
-__device__ __forceinline__ void publish_step(StepCtrl* c, int p, const LoopParams& lp, bool done, double dt) {
+// clear_next = false in a one-launch 1D step, whose other blocks may already
+// be adding to slot q (its last block writes maxs[q][0]).
+__device__ __forceinline__ void publish_step(StepCtrl* c, int p, const LoopParams& lp, bool done, double dt,
+                                             bool clear_next = true) {
     int q = p ^ 1;
     if (done) {
         c->active[p] = 0;
@@ -146,8 +181,10 @@ __device__ __forceinline__ void publish_step(StepCtrl* c, int p, const LoopParam
     c->dt[p] = dt;
     c->time[q] = c->time[p] + dt;
     c->step[q] = c->step[p] + 1;
-    c->maxs[q][0] = 0ull;
-    c->maxs[q][1] = 0ull;
+    if (clear_next) {
+        c->maxs[q][0] = 0ull;
+        c->maxs[q][1] = 0ull;
+    }
     int s = c->step[p];
     if (lp.dts_out && s < lp.dts_cap) lp.dts_out[s] = dt;
 }

@@ -558,4 +558,9 @@ cudaError_t launch_1d_step(double* U, double* U1, int n, int h, double dx, doubl
     return launch_1d_step_t<double>(U, U1, n, h, dx, gamma, bc, lp, ctrl, p, which, st, Uout);
 }
 
+cudaError_t launch_1d_fused(const double* Un, double* Unext, double* U1out, int n, int h, double dx, double gamma,
+                            int bc, const LoopParams& lp, StepCtrl* ctrl, int p, cudaStream_t st) {
+    return launch_1d_fused_t<double>(Un, Unext, U1out, n, h, dx, gamma, bc, lp, ctrl, p, st);
+}
+
 }  // namespace nestb

@@ -15,4 +15,9 @@ cudaError_t launch_1d_step_f32(float* U, float* U1, int n, int h, double dx, dou
     return launch_1d_step_t<float>(U, U1, n, h, dx, gamma, bc, lp, ctrl, p, which, st, Uout);
 }
 
+cudaError_t launch_1d_fused_f32(const float* Un, float* Unext, float* U1out, int n, int h, double dx, double gamma,
+                               int bc, const LoopParams& lp, StepCtrl* ctrl, int p, cudaStream_t st) {
+    return launch_1d_fused_t<float>(Un, Unext, U1out, n, h, dx, gamma, bc, lp, ctrl, p, st);
+}
+
 }  // namespace nestb

@@ -9,7 +9,8 @@
 // copies it feeds; stage 2 fuses the Heun average and the block's max
 // |u|+c (one atomic per block).  dt is derived on the device from that
 // maximum by the next stage 1, so a step is two launches and no host
-// synchronisation.
+// synchronisation.  k1d_step runs a whole step in one launch (out of place),
+// recomputing the stage-1 halo per CTA.
 #pragma once
 
 #include "common.cuh"
@@ -18,7 +19,9 @@
 namespace nestb {
 namespace {
 
-constexpr int T1 = 256;       // cells per tile
+// cells per tile: 224 puts at most 448 cells on an SM at 65536 cells (293
+// tiles over 148 SMs; 256 gave 512 on most SMs): FP64 step 8.76 -> 8.46 us
+constexpr int T1 = 224;
 // threads per block: at least one per extended cell (T1 + 4), so that no
 // phase loops twice, in whole warps (the stage-2 reduction shuffles over
 // full warps)
@@ -53,6 +56,8 @@ k1d_stage(const T* __restrict__ Uin, const T* Un, T* Uout,
     __shared__ T W[3][T1 + 4];
     __shared__ T F[3][T1 + 1];
     __shared__ double red[33];
+    pdl_wait();
+    pdl_trigger();
     int nt = n + 2 * h;
     const T gamma = (T)gamma_d;
     const T gm1 = (T)(gamma_d - 1.0);
@@ -135,12 +140,175 @@ k1d_stage(const T* __restrict__ Uin, const T* Un, T* Uout,
     }
 }
 
+// Interior cell whose value cell c holds (any c, ghost cells and beyond
+// included): nest's periodic copy, or the zero-gradient copy of the nearest
+// end cell.
+__device__ __forceinline__ int source_cell_1d(int c, int n, int bc) {
+    if (bc == BC_PERIODIC) {
+        c %= n;
+        return c < 0 ? c + n : c;
+    }
+    return min(max(c, 0), n - 1);
+}
+
+// One whole RK2 (Heun) step in one launch, out of place (Un -> Unext; the
+// caller alternates two buffers).  A CTA owns T1 cells and keeps everything
+// of its step in shared memory:
+//   U^n and its primitives over the cells c0-4 .. c0+T1+3,
+//   the stage-1 faces and U1 over c0-2 .. c0+T1+1 (the 2-cell halo of U1 is
+//   recomputed here instead of being exchanged through global memory),
+//   the primitives of U1, the stage-2 faces and the Heun update of the T1
+//   cells, the new state's ghost copies, positivity check and max |u|+c.
+// Every value is computed by the same expression, on the same operands, as in
+// the two stage kernels (and nest's loop): U1 of a ghost cell is U1 of the
+// cell it copies, which the periodic wrap of the primitives gives directly
+// and the zero-gradient case takes from that cell's faces.  The wave-speed
+// maximum is reduced into maxs[q][1]; the last block to finish moves it to
+// maxs[q][0] (block 0 cannot clear a slot at its start that other blocks may
+// already be adding to).  U1out (optional) receives U1 of the step with its
+// ghosts.  A finished step (time, step count or error) copies Un to Unext so
+// that the state ends in the buffer the caller expects.
+template <typename T>
+__global__ void __launch_bounds__(NT1)
+k1d_step(const T* __restrict__ Un, T* __restrict__ Unext, T* __restrict__ U1out, int n, int h, double dx,
+         double gamma_d, int bc, LoopParams lp, StepCtrl* ctrl, int p) {
+    __shared__ T Q[3][T1 + 8];  // U^n, cells c0-4 ..
+    __shared__ T W[3][T1 + 8];  // primitives of U^n (cells c0-4 ..), then of U1 (cells c0-2 ..)
+    __shared__ T F[3][T1 + 5];  // faces of the stage
+    __shared__ T V[3][T1 + 4];  // U1, cells c0-2 ..
+    __shared__ double red[NT1 / 32];
+    pdl_wait();
+    pdl_trigger();
+    const int nt = n + 2 * h;
+    const T gamma = (T)gamma_d;
+    const T gm1 = (T)(gamma_d - 1.0);
+    const int c0 = blockIdx.x * T1;
+    if (step_is_done(ctrl, p, lp)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) publish_step(ctrl, p, lp, true, 0.0, false);
+        for (int t = threadIdx.x; t < T1; t += NT1) {
+            const int c = c0 + t;
+            if (c < n)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const T v = Un[k * nt + h + c];
+                    Unext[k * nt + h + c] = v;
+                    push_ghosts_1d(Unext, nt, k, c, n, h, bc, v);
+                }
+        }
+        return;
+    }
+    double dt;
+    {
+        const double pd = prescribed_dt(ctrl, p, lp);
+        if (pd > 0.0) {
+            dt = pd;
+        } else {
+            dt = lp.cfl * dx / bits_speed(ctrl->maxs[p][0]);
+            if (lp.t_final > 0.0) dt = smin(dt, lp.t_final - ctrl->time[p]);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) publish_step(ctrl, p, lp, false, dt, false);
+    const T dtdx = (T)(dt / dx);
+
+    // U^n and its primitives, cells c0-4+t (read from the interior cell each copies)
+    for (int t = threadIdx.x; t < T1 + 8; t += NT1) {
+        const int e = h + source_cell_1d(c0 - 4 + t, n, bc);
+        const T rho = Un[e], mom = Un[nt + e], erg = Un[2 * nt + e];
+        Q[0][t] = rho; Q[1][t] = mom; Q[2][t] = erg;
+        W[0][t] = rho;
+        W[1][t] = mom / rho;
+        W[2][t] = eos_pressure(gm1, rho, mom, erg);
+    }
+    __syncthreads();
+    // face f between the cells of W slots f+1 and f+2
+    auto faces = [&](int nf) {
+        for (int f = threadIdx.x; f < nf; f += NT1) {
+            const int a = f + 1, b = f + 2;
+            T sa[3], sb[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                sa[k] = limit(W[k][a] - W[k][a - 1], W[k][b] - W[k][a], lp.lim);
+                sb[k] = limit(W[k][b] - W[k][a], W[k][b + 1] - W[k][b], lp.lim);
+            }
+            T f0, f1, f2;
+            hlle1d(gamma, gm1, W[0][a] + T(0.5) * sa[0], W[1][a] + T(0.5) * sa[1], W[2][a] + T(0.5) * sa[2],
+                   W[0][b] - T(0.5) * sb[0], W[1][b] - T(0.5) * sb[1], W[2][b] - T(0.5) * sb[2], f0, f1, f2);
+            F[0][f] = f0; F[1][f] = f1; F[2][f] = f2;
+        }
+    };
+    faces(T1 + 5);  // stage 1: faces between cells c0-3+f and c0-2+f
+    __syncthreads();
+    // U1 of cells c0-2+u (faces u, u+1; U^n slot u+2) and its primitives into W slot u
+    for (int u = threadIdx.x; u < T1 + 4; u += NT1) {
+        // zero-gradient ghost: the value of the end cell it copies, which lies
+        // in this window whenever the window reaches past the domain
+        const int us = bc == BC_PERIODIC ? u : source_cell_1d(c0 - 2 + u, n, bc) - c0 + 2;
+        T v[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            v[k] = Q[k][us + 2] - dtdx * (F[k][us + 1] - F[k][us]);
+            V[k][u] = v[k];
+        }
+        W[0][u] = v[0];
+        W[1][u] = v[1] / v[0];
+        W[2][u] = eos_pressure(gm1, v[0], v[1], v[2]);
+    }
+    __syncthreads();
+    faces(T1 + 1);  // stage 2: faces between cells c0-1+f and c0+f
+    __syncthreads();
+    const int t = threadIdx.x, c = c0 + t;
+    double ms = 0.0;
+    if (t < T1 && c < n) {
+        const int e = h + c;
+        T v[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const T s = V[k][t + 2] - dtdx * (F[k][t + 1] - F[k][t]);
+            v[k] = T(0.5) * (Q[k][t + 4] + s);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            Unext[k * nt + e] = v[k];
+            push_ghosts_1d(Unext, nt, k, c, n, h, bc, v[k]);
+            if (U1out) {
+                U1out[k * nt + e] = V[k][t + 2];
+                push_ghosts_1d(U1out, nt, k, c, n, h, bc, V[k][t + 2]);
+            }
+        }
+        T pr;
+        ms = (double)cell_speed_1d(v[0], v[1], v[2], gamma, gm1, pr);
+        if (!(v[0] > T(0)) || !(pr > T(0))) flag_cell(ctrl, ctrl->step[p] + 1, (double)v[0], (double)pr, c, 0);
+    }
+    ms = warp_max(ms);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = ms;
+    __syncthreads();
+    if (w == 0) {
+        double x = (l < NT1 / 32) ? red[l] : 0.0;
+        x = warp_max(x);
+        if (l == 0) {
+            const int q = p ^ 1;
+            if (!(x == x) || x > 1.79e308) atomicOr(&ctrl->err, ERRW_NONFINITE);
+            atomic_max_speed(&ctrl->maxs[q][1], x);
+            __threadfence();
+            if (atomicAdd(&ctrl->blocks_done, 1u) == gridDim.x - 1) {
+                // every block has added its maximum
+                __threadfence();
+                ctrl->maxs[q][0] = atomicExch(&ctrl->maxs[q][1], 0ull);
+                ctrl->blocks_done = 0u;
+            }
+        }
+    }
+}
+
 // Ghost fill + max |u|+c of the current state into slot p (used once after
 // an upload, and by the standalone compute_dt entry point).
 template <typename T>
 __global__ void __launch_bounds__(T1)
 k1d_prepare(T* U, int n, int h, double gamma_d, int bc, StepCtrl* ctrl, int p) {
     __shared__ double red[33];
+    pdl_wait();
+    pdl_trigger();
     int nt = n + 2 * h;
     const T gamma = (T)gamma_d;
     const T gm1 = (T)(gamma_d - 1.0);
@@ -169,17 +337,28 @@ k1d_prepare(T* U, int n, int h, double gamma_d, int bc, StepCtrl* ctrl, int p) {
 template <typename T>
 cudaError_t launch_1d_prepare_t(T* U, int n, int h, double gamma, int bc, StepCtrl* ctrl, int p, cudaStream_t st) {
     int blocks = (n + T1 - 1) / T1;
-    k1d_prepare<T><<<blocks, T1, 0, st>>>(U, n, h, gamma, bc, ctrl, p);
-    return cudaGetLastError();
+    return launch_pdl(k1d_prepare<T>, dim3(blocks), dim3(T1), 0, st, U, n, h, gamma, bc, ctrl, p);
 }
 
 template <typename T>
 cudaError_t launch_1d_step_t(T* U, T* U1, int n, int h, double dx, double gamma, int bc, const LoopParams& lp,
                              StepCtrl* ctrl, int p, int which, cudaStream_t st, T* Uout) {
     int blocks = (n + T1 - 1) / T1;
-    if (which & 1) k1d_stage<T, 1><<<blocks, NT1, 0, st>>>(U, nullptr, U1, n, h, dx, gamma, bc, lp, ctrl, p);
-    if (which & 2) k1d_stage<T, 2><<<blocks, NT1, 0, st>>>(U1, U, Uout ? Uout : U, n, h, dx, gamma, bc, lp, ctrl, p);
-    return cudaGetLastError();
+    cudaError_t e = cudaSuccess;
+    if (which & 1)
+        e = launch_pdl(k1d_stage<T, 1>, dim3(blocks), dim3(NT1), 0, st, (const T*)U, (const T*)nullptr, U1, n, h, dx,
+                       gamma, bc, lp, ctrl, p);
+    if ((which & 2) && e == cudaSuccess)
+        e = launch_pdl(k1d_stage<T, 2>, dim3(blocks), dim3(NT1), 0, st, (const T*)U1, (const T*)U, Uout ? Uout : U, n,
+                       h, dx, gamma, bc, lp, ctrl, p);
+    return e;
+}
+
+template <typename T>
+cudaError_t launch_1d_fused_t(const T* Un, T* Unext, T* U1out, int n, int h, double dx, double gamma, int bc,
+                              const LoopParams& lp, StepCtrl* ctrl, int p, cudaStream_t st) {
+    int blocks = (n + T1 - 1) / T1;
+    return launch_pdl(k1d_step<T>, dim3(blocks), dim3(NT1), 0, st, Un, Unext, U1out, n, h, dx, gamma, bc, lp, ctrl, p);
 }
 
 }  // namespace

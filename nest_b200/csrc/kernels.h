@@ -28,12 +28,19 @@ cudaError_t launch_1d_prepare(double* U, int n, int h, double gamma, int bc, Ste
 cudaError_t launch_1d_step(double* U, double* U1, int n, int h, double dx, double gamma, int bc,
                            const LoopParams& lp, StepCtrl* ctrl, int p, int which, cudaStream_t st,
                            double* Uout = nullptr);
+// One whole step in one launch, out of place: Un -> Unext (distinct buffers;
+// the caller alternates them), U1 of the step into U1out when not null.  The
+// same values as the two stage launches, bit for bit.
+cudaError_t launch_1d_fused(const double* Un, double* Unext, double* U1out, int n, int h, double dx, double gamma,
+                            int bc, const LoopParams& lp, StepCtrl* ctrl, int p, cudaStream_t st);
 // 1D FP32 form (tiled kernels only; time, dt and wave speeds in FP64).
 cudaError_t launch_1d_prepare_f32(float* U, int n, int h, double gamma, int bc, StepCtrl* ctrl, int p,
                                   cudaStream_t st);
 cudaError_t launch_1d_step_f32(float* U, float* U1, int n, int h, double dx, double gamma, int bc,
                                const LoopParams& lp, StepCtrl* ctrl, int p, int which, cudaStream_t st,
                                float* Uout = nullptr);
+cudaError_t launch_1d_fused_f32(const float* Un, float* Unext, float* U1out, int n, int h, double dx, double gamma,
+                               int bc, const LoopParams& lp, StepCtrl* ctrl, int p, cudaStream_t st);
 
 // 2D unsplit scheme.  `which`: 1 = stage 1, 2 = stage 2, 3 = both.
 cudaError_t launch_2d_prepare_f64(double* U, const Geo2D& g, StepCtrl* ctrl, int p, cudaStream_t st);

@@ -5,8 +5,8 @@
 // cudaMalloc, plugin hosts that sandbox device allocations, and real-time
 // loops that must not pay allocation latency (or risk an allocation failure)
 // after start-up.  nest_euler1d_run_noalloc serves them: the caller passes the
-// state buffer, and the solver's scratch -- the stage buffer U1 and the step
-// control block -- lives in a fixed file-scope device array below, so the
+// state buffer, and the solver's scratch -- a second state buffer U1 and the
+// step control block -- lives in a fixed file-scope device array below, so the
 // call itself never allocates or frees memory.
 //
 // The array is part of the library image: every GPU that loads the library
@@ -86,8 +86,14 @@ extern "C" nest_status nest_euler1d_run_noalloc(double* d_state, int n_interior,
     const int chunk = 32;
     int last_step = -1;
     while (e == cudaSuccess) {
-        for (int i = 0; i < chunk && e == cudaSuccess; ++i, parity ^= 1)
-            e = nestb::launch_1d_step(d_state, U1, n_interior, n_halo, dx, gamma, bc, lp, ctrl, parity, 3, st);
+        // one launch per step, out of place: d_state -> U1 -> d_state (the
+        // chunk is even, so the state ends in the caller's buffer)
+        for (int i = 0; i < chunk && e == cudaSuccess; i += 2) {
+            e = nestb::launch_1d_fused(d_state, U1, nullptr, n_interior, n_halo, dx, gamma, bc, lp, ctrl, parity, st);
+            if (e == cudaSuccess)
+                e = nestb::launch_1d_fused(U1, d_state, nullptr, n_interior, n_halo, dx, gamma, bc, lp, ctrl,
+                                           parity ^ 1, st);
+        }
         if (e == cudaSuccess) e = cudaMemcpyAsync(&host, ctrl, sizeof host, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) break;

@@ -49,7 +49,8 @@ def test_run_to_matches_oracle(gpu, oracle, n, bc, cfl, tf, resident):
 
 
 @pytest.mark.parametrize("n", [4, 255, 256, 257, 4099, 70001])
-def test_tiled_fixed_steps_ragged(gpu, oracle, n):
+@pytest.mark.parametrize("bc", [BC_PERIODIC, BC_OUTFLOW])
+def test_tiled_fixed_steps_ragged(gpu, oracle, n, bc):
     rng = np.random.default_rng(n)
     x = np.arange(n + 4)
     rho = 1.0 + 0.3 * np.sin(2 * np.pi * x / max(n, 8)) + 0.05 * rng.random(n + 4)
@@ -57,12 +58,40 @@ def test_tiled_fixed_steps_ragged(gpu, oracle, n):
     p = 1.0 + 0.2 * rng.random(n + 4)
     U = np.stack([rho, rho * u, p / 0.4 + 0.5 * rho * u * u])
     want = U.copy()
-    oracle.run1d(want, n, 2, 1.0 / n, G, 0.5, nsteps=23, bc=BC_PERIODIC)
-    s = gpu.Solver(1, n, bc=BC_PERIODIC, flags=gpu.FLAG_NO_RESIDENT)
+    oracle.run1d(want, n, 2, 1.0 / n, G, 0.5, nsteps=23, bc=bc)
+    s = gpu.Solver(1, n, bc=bc, flags=gpu.FLAG_NO_RESIDENT)
     s.upload(U)
     s.step(23, 0.5)
     got = s.download()
     assert np.array_equal(got[:, 2:-2], want[:, 2:-2])
+
+
+@pytest.mark.parametrize("bc", [BC_PERIODIC, BC_OUTFLOW])
+def test_step_sequences_mix_launch_forms(gpu, oracle, bc):
+    """Tiled steps go in pairs of one-launch steps (U -> U1 -> U, the stage-1
+    halo recomputed per block) and an odd last step runs the two stage
+    launches in place; any sequence of calls, with CFL dt from the wave
+    speeds each form leaves behind, follows the oracle bit for bit."""
+    n = 9001  # past the cluster form: tiled path
+    U = sod_ic_1d(n)
+    want = U.copy()
+    s = gpu.Solver(1, n, bc=bc)
+    s.upload(U)
+    total = 0
+    for k in [1, 2, 3, 16, 5, 33, 1]:
+        s.step(k, 0.4)
+        total += k
+    wsteps, wt, _ = oracle.run1d(want, n, 2, 1.0 / n, G, 0.4, nsteps=total, bc=bc)
+    t, steps = s.time()
+    assert steps == wsteps == total and t == wt
+    assert np.array_equal(s.download()[:, 2:-2], want[:, 2:-2])
+    # a stopping time inside a pair: the finished step passes the state on unchanged
+    tf = t + 2.5 * (wt / total)
+    k = s.run_to(tf, 0.4)
+    want = U.copy()
+    wall, wtf, _ = oracle.run1d(want, n, 2, 1.0 / n, G, 0.4, t_final=tf, bc=bc)
+    assert k == wall - total and s.time() == (wtf, wall)
+    assert np.array_equal(s.download()[:, 2:-2], want[:, 2:-2])
 
 
 def test_compute_dt_and_rk2_step(gpu, oracle):
