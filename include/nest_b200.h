@@ -338,13 +338,13 @@ nest_status nest_adjoint_stats(nest_adjoint* a, double* fwd_ms, double* bwd_ms, 
 /* For callers that cannot allocate device memory (a host code that owns    */
 /* the whole GPU through its own pool, a plugin host that forbids library   */
 /* allocations, a real-time loop that must not allocate after start-up).    */
-/* The caller passes the state; the solver's scratch (stage buffer and      */
-/* control block) is a fixed array inside the library, so this call makes   */
-/* no cudaMalloc / cudaFree.  The array holds n_interior + 2*n_halo <=      */
-/* NEST_NOALLOC_MAX_CELLS cells (about 1.6 MB, held by every GPU that loads */
-/* the library until exit); larger sizes return NEST_ERR_INVALID.  Every    */
-/* call looks up the array's address in the current device's context and    */
-/* waits for its stream (it reads the step count back every 32 steps).      */
+/* The caller passes the state; the solver's scratch (a second state buffer */
+/* and the control block) is a fixed array inside the library, so this call */
+/* makes no cudaMalloc / cudaFree.  The array holds n_interior + 2*n_halo   */
+/* <= NEST_NOALLOC_MAX_CELLS cells (about 1.6 MB, held by every GPU that    */
+/* loads the library until exit); larger sizes return NEST_ERR_INVALID.     */
+/* Every call looks up the array's address in the current device's context  */
+/* and waits for its stream (it reads the step count back every 32 steps).  */
 /* All calls share the array: calls that overlap on the GPU race.           */
 /*                                                                          */
 /* d_state: device SoA [var * n_total + i], n_total = n_interior + 2 n_halo */

@@ -4,8 +4,8 @@ Some callers cannot allocate device memory: a host code that owns the whole
 GPU through its own memory pool, a plugin host that forbids libraries from
 allocating, a real-time loop that must not allocate after start-up.  For them
 the library offers one entry point that takes the caller's state buffer and
-keeps its own scratch (stage buffer and step control block) in a fixed array
-inside the library, so the call makes no allocation.
+keeps its own scratch (a second state buffer and the step control block) in a
+fixed array inside the library, so the call makes no allocation.
 
 The test calls it through the C ABI twice in a row, each time comparing the
 result with the allocating entry points (euler1d_gpu_run / nest_solver_run_to)
