@@ -268,7 +268,7 @@ def kernel_name(form: str, stage: str) -> str:
         return "k2d_f32x2<1, true, false>" if stage == "stage1" else "k2d_f32x2<2, true, true>"
     if form == "f32plain":
         return f"k2d_f32x2<{stage[-1]}, false, false>"
-    return f"k2d_f64r<{stage[-1]}, 0>"
+    return f"k2d_f64r<{stage[-1]}, 0, 0>"  # minmod instance
 
 
 def traffic_from_profiles(form: str, n: int):

@@ -49,7 +49,9 @@ __device__ __forceinline__ void push_ghosts_1d(T* U, int nt, int k, int c, int n
     }
 }
 
-template <typename T, int STAGE>
+// LIM (both kernels): the slope limiter fixed at compile time (LIM_MINMOD,
+// nest's default) or -1 to read it from the loop parameters.
+template <typename T, int STAGE, int LIM>
 __global__ void __launch_bounds__(NT1)
 k1d_stage(const T* __restrict__ Uin, const T* Un, T* Uout,
           int n, int h, double dx, double gamma_d, int bc, LoopParams lp, StepCtrl* ctrl, int p) {
@@ -94,8 +96,8 @@ k1d_stage(const T* __restrict__ Uin, const T* Un, T* Uout,
         T sa[3], sb[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            sa[k] = limit(W[k][a] - W[k][a - 1], W[k][b] - W[k][a], lp.lim);
-            sb[k] = limit(W[k][b] - W[k][a], W[k][b + 1] - W[k][b], lp.lim);
+            sa[k] = limit(W[k][a] - W[k][a - 1], W[k][b] - W[k][a], LIM >= 0 ? LIM : lp.lim);
+            sb[k] = limit(W[k][b] - W[k][a], W[k][b + 1] - W[k][b], LIM >= 0 ? LIM : lp.lim);
         }
         T f0, f1, f2;
         hlle1d(gamma, gm1, W[0][a] + T(0.5) * sa[0], W[1][a] + T(0.5) * sa[1], W[2][a] + T(0.5) * sa[2],
@@ -168,7 +170,7 @@ __device__ __forceinline__ int source_cell_1d(int c, int n, int bc) {
 // already be adding to).  U1out (optional) receives U1 of the step with its
 // ghosts.  A finished step (time, step count or error) copies Un to Unext so
 // that the state ends in the buffer the caller expects.
-template <typename T>
+template <typename T, int LIM>
 __global__ void __launch_bounds__(NT1)
 k1d_step(const T* __restrict__ Un, T* __restrict__ Unext, T* __restrict__ U1out, int n, int h, double dx,
          double gamma_d, int bc, LoopParams lp, StepCtrl* ctrl, int p) {
@@ -227,8 +229,8 @@ k1d_step(const T* __restrict__ Un, T* __restrict__ Unext, T* __restrict__ U1out,
             T sa[3], sb[3];
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                sa[k] = limit(W[k][a] - W[k][a - 1], W[k][b] - W[k][a], lp.lim);
-                sb[k] = limit(W[k][b] - W[k][a], W[k][b + 1] - W[k][b], lp.lim);
+                sa[k] = limit(W[k][a] - W[k][a - 1], W[k][b] - W[k][a], LIM >= 0 ? LIM : lp.lim);
+                sb[k] = limit(W[k][b] - W[k][a], W[k][b + 1] - W[k][b], LIM >= 0 ? LIM : lp.lim);
             }
             T f0, f1, f2;
             hlle1d(gamma, gm1, W[0][a] + T(0.5) * sa[0], W[1][a] + T(0.5) * sa[1], W[2][a] + T(0.5) * sa[2],
@@ -344,13 +346,14 @@ template <typename T>
 cudaError_t launch_1d_step_t(T* U, T* U1, int n, int h, double dx, double gamma, int bc, const LoopParams& lp,
                              StepCtrl* ctrl, int p, int which, cudaStream_t st, T* Uout) {
     int blocks = (n + T1 - 1) / T1;
+    const bool mm = lp.lim == LIM_MINMOD;
     cudaError_t e = cudaSuccess;
     if (which & 1)
-        e = launch_pdl(k1d_stage<T, 1>, dim3(blocks), dim3(NT1), 0, st, (const T*)U, (const T*)nullptr, U1, n, h, dx,
-                       gamma, bc, lp, ctrl, p);
+        e = launch_pdl(mm ? k1d_stage<T, 1, LIM_MINMOD> : k1d_stage<T, 1, -1>, dim3(blocks), dim3(NT1), 0, st,
+                       (const T*)U, (const T*)nullptr, U1, n, h, dx, gamma, bc, lp, ctrl, p);
     if ((which & 2) && e == cudaSuccess)
-        e = launch_pdl(k1d_stage<T, 2>, dim3(blocks), dim3(NT1), 0, st, (const T*)U1, (const T*)U, Uout ? Uout : U, n,
-                       h, dx, gamma, bc, lp, ctrl, p);
+        e = launch_pdl(mm ? k1d_stage<T, 2, LIM_MINMOD> : k1d_stage<T, 2, -1>, dim3(blocks), dim3(NT1), 0, st,
+                       (const T*)U1, (const T*)U, Uout ? Uout : U, n, h, dx, gamma, bc, lp, ctrl, p);
     return e;
 }
 
@@ -358,7 +361,8 @@ template <typename T>
 cudaError_t launch_1d_fused_t(const T* Un, T* Unext, T* U1out, int n, int h, double dx, double gamma, int bc,
                               const LoopParams& lp, StepCtrl* ctrl, int p, cudaStream_t st) {
     int blocks = (n + T1 - 1) / T1;
-    return launch_pdl(k1d_step<T>, dim3(blocks), dim3(NT1), 0, st, Un, Unext, U1out, n, h, dx, gamma, bc, lp, ctrl, p);
+    return launch_pdl(lp.lim == LIM_MINMOD ? k1d_step<T, LIM_MINMOD> : k1d_step<T, -1>, dim3(blocks), dim3(NT1), 0, st,
+                      Un, Unext, U1out, n, h, dx, gamma, bc, lp, ctrl, p);
 }
 
 }  // namespace

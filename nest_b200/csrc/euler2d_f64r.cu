@@ -49,7 +49,10 @@ __device__ __forceinline__ W4 half_back(const W4& w, const W4& s) {
     return { w.a - 0.5 * s.a, w.b - 0.5 * s.b, w.c - 0.5 * s.c, w.d - 0.5 * s.d };
 }
 
-template <int STAGE, bool TOT>
+// LIM: the slope limiter fixed at compile time (LIM_MINMOD, nest's default),
+// or -1 to read it from the loop parameters; a fixed limiter leaves no
+// limiter branch in the row loop.
+template <int STAGE, bool TOT, int LIM>
 __device__ __forceinline__ void f64r_body(const StageArgs<double>& a, int strip, int tile_row) {
     const Geo2D& g = a.g;
     const int lane = threadIdx.x & 31;
@@ -76,7 +79,7 @@ __device__ __forceinline__ void f64r_body(const StageArgs<double>& a, int strip,
     }
     const double dtdx = dt / g.dx;
     const double dtdy = dt / g.dy;
-    const int lim = a.lp.lim;
+    const int lim = LIM >= 0 ? LIM : a.lp.lim;
 
     const int nx = g.nx, ny = g.ny, pitch = g.pitch;
     const int j0 = strip * STRIP;
@@ -245,9 +248,19 @@ __device__ __forceinline__ void f64r_body(const StageArgs<double>& a, int strip,
 #define NEST_F64R_ATTR __launch_bounds__(256)
 #endif
 
-template <int STAGE, bool TOT>
+template <int STAGE, bool TOT, int LIM>
 __global__ void NEST_F64R_ATTR k2d_f64r(StageArgs<double> a) {
-    f64r_body<STAGE, TOT>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+    f64r_body<STAGE, TOT, LIM>(a, blockIdx.x * blockDim.y + threadIdx.y, blockIdx.y);
+}
+
+template <int LIM>
+void launch_f64r_lim(const StageArgs<double>& a1, const StageArgs<double>& a2, dim3 gr, dim3 b, size_t sm1,
+                     size_t sm2, int which, bool tot, cudaStream_t st) {
+    if (which & 1) k2d_f64r<1, false, LIM><<<gr, b, sm1, st>>>(a1);
+    if (which & 2) {
+        if (tot) k2d_f64r<2, true, LIM><<<gr, b, sm2, st>>>(a2);
+        else k2d_f64r<2, false, LIM><<<gr, b, sm2, st>>>(a2);
+    }
 }
 
 size_t f64r_ring_bytes(int stage, int warps) { return (size_t)warps * ring_d_per_warp(stage) * sizeof(double); }
@@ -262,11 +275,8 @@ cudaError_t launch_2d_step_f64r(double* U, double* U1, const Geo2D& g, const Loo
     StageArgs<double> a1{U, nullptr, U1, g, lp, ctrl, nullptr, p, tx};
     StageArgs<double> a2{U1, U, Uout ? Uout : U, g, lp, ctrl, partials, p, tx};
     const size_t sm1 = f64r_ring_bytes(1, warps), sm2 = f64r_ring_bytes(2, warps);
-    if (which & 1) k2d_f64r<1, false><<<gr, b, sm1, st>>>(a1);
-    if (which & 2) {
-        if (partials) k2d_f64r<2, true><<<gr, b, sm2, st>>>(a2);
-        else k2d_f64r<2, false><<<gr, b, sm2, st>>>(a2);
-    }
+    if (lp.lim == LIM_MINMOD) launch_f64r_lim<LIM_MINMOD>(a1, a2, gr, b, sm1, sm2, which, partials != nullptr, st);
+    else launch_f64r_lim<-1>(a1, a2, gr, b, sm1, sm2, which, partials != nullptr, st);
     return cudaGetLastError();
 }
 
