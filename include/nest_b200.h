@@ -333,6 +333,15 @@ nest_status nest_adjoint_stats(nest_adjoint* a, double* fwd_ms, double* bwd_ms, 
                                long long* snapshot_bytes);
 
 /* ------------------------------------------------------------------------ */
+/* Self-test of the FP64 stage kernels' checked division.  No counterpart   */
+/* in nest.  For n pairs (device arrays), q[i] = the fast quotient of       */
+/* a[i] / b[i] and ok[i] = 1 where the kernels accept it as the correctly   */
+/* rounded IEEE quotient (0 where they fall back to the IEEE division).     */
+/* Enqueued on the legacy stream; synchronises before returning.            */
+/* ------------------------------------------------------------------------ */
+nest_status nest_selftest_div_f64(const double* d_a, const double* d_b, double* d_q, int* d_ok, int n);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free 1D run.  No counterpart in nest's ABI.                   */
 /*                                                                          */
 /* For callers that cannot allocate device memory (a host code that owns    */

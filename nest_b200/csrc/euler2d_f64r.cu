@@ -15,10 +15,12 @@
 // A warp owns a strip of 32 columns j0-2 .. j0+29 (j0 = 28 strip) and
 // writes lanes 2..29, like stage2d_body.
 #include "euler2d_kernels.cuh"
+#include "f64div.cuh"
 #include "kernels.h"
 
 #include <algorithm>
 #include <cstdlib>
+#include <string>
 
 namespace nestb {
 namespace {
@@ -47,6 +49,67 @@ __device__ __forceinline__ W4 half_step(const W4& w, const W4& s, double h) {
 }
 __device__ __forceinline__ W4 half_back(const W4& w, const W4& s) {
     return { w.a - 0.5 * s.a, w.b - 0.5 * s.b, w.c - 0.5 * s.c, w.d - 0.5 * s.d };
+}
+
+// Division policies of a row: the IEEE division, or the checked fast
+// division of f64div.cuh, which returns the same value whenever it leaves
+// `ok` set (a row with any cleared flag in the warp is recomputed with the
+// IEEE policy before anything of it is stored).
+struct DivIeee {
+    __device__ __forceinline__ double div(double x, double y) { return x / y; }
+};
+struct DivChecked {
+    bool ok = true;
+    __device__ __forceinline__ double div(double x, double y) { return div_rn_checked(x, y, ok); }
+};
+
+// cons2prim, hlle4 and cell_speeds_p of euler2d_kernels.cuh for the FP64
+// plain form (the same expressions in the same order, so the same values),
+// with their divisions taken from a policy.
+template <class D>
+__device__ __forceinline__ W4 prim_d(D& d, const W4& c, double gm1) {
+    const double u = d.div(c.b, c.a), v = d.div(c.c, c.a);
+    const double p = gm1 * (c.d - ke2(c.a, u, v));
+    return { c.a, u, v, smax(p, 0.0) };
+}
+
+template <class D>
+__device__ __forceinline__ void hlle4_d(D& d, double gamma, double gm1, double rL, double nL, double tL, double pL,
+                                        double rR, double nR, double tR, double pR, double& f0, double& f1,
+                                        double& f2, double& f3) {
+    const double cL = sqrt(d.div(gamma * pL, rL));
+    const double cR = sqrt(d.div(gamma * pR, rR));
+    const double EL = d.div(pL, gm1) + ke2(rL, nL, tL);
+    const double ER = d.div(pR, gm1) + ke2(rR, nR, tR);
+    const double SL = smin(nL - cL, nR - cR);
+    const double SR = smax(nL + cL, nR + cR);
+    const double mL = rL * nL, mR = rR * nR;
+    const double FL0 = mL, FL1 = mL * nL + pL, FL2 = mL * tL, FL3 = (EL + pL) * nL;
+    const double FR0 = mR, FR1 = mR * nR + pR, FR2 = mR * tR, FR3 = (ER + pR) * nR;
+    if (SL >= 0.0) {
+        f0 = FL0; f1 = FL1; f2 = FL2; f3 = FL3;
+    } else if (SR <= 0.0) {
+        f0 = FR0; f1 = FR1; f2 = FR2; f3 = FR3;
+    } else {
+        const double SLR = SL * SR, dS = SR - SL;
+        f0 = d.div(SR * FL0 - SL * FR0 + SLR * (rR - rL), dS);
+        f1 = d.div(SR * FL1 - SL * FR1 + SLR * (mR - mL), dS);
+        f2 = d.div(SR * FL2 - SL * FR2 + SLR * (rR * tR - rL * tL), dS);
+        f3 = d.div(SR * FL3 - SL * FR3 + SLR * (ER - EL), dS);
+    }
+}
+
+template <class D>
+__device__ __forceinline__ double speeds_d(D& d, double U0, double U1, double U2, double U3, double gamma,
+                                           double gm1, double& sx, double& sy) {
+    const double rho = smax(U0, 1e-10);
+    const double u = d.div(U1, rho), v = d.div(U2, rho);
+    const double ke = 0.5 * rho * (u * u + v * v);
+    const double p = smax(gm1 * (U3 - ke), 1e-10);
+    const double c = sqrt(d.div(gamma * p, rho));
+    sx = fabs(u) + c;
+    sy = fabs(v) + c;
+    return gm1 * (U3 - ke2(rho, u, v));
 }
 
 // LIM: the slope limiter fixed at compile time (LIM_MINMOD, nest's default),
@@ -161,48 +224,73 @@ __device__ __forceinline__ void f64r_body(const StageArgs<double>& a, int strip,
         cpd_wait<LOOKD - 2>();
         __syncwarp();
 
-        // x-face i+1/2 from rows i .. i+2
-        const W4 W2 = prim(ring_row(i + 2));
-        const W4 S1 = limit4(Wq, Wq1, W2, lim);
-        const W4 M1 = half_back(Wq1, S1);
-        W4 Fc;
-        hlle4<double>(gamma, gm1, igm1, Pq.a, Pq.b, Pq.c, Pq.d, M1.a, M1.b, M1.c, M1.d, Fc.a, Fc.b, Fc.c, Fc.d);
-
-        // y-faces on row i: face j+1/2 (normal v, transverse u), the left
-        // face from the left neighbour
-        const W4 sy = limit4(shfl_up4(Wq), Wq, shfl_dn4(Wq), lim);
-        const W4 Rq = shfl_dn4(half_back(Wq, sy));
-        const W4 Ly = half_step(Wq, sy, 0.5);
-        W4 Gy;
-        hlle4<double>(gamma, gm1, igm1, Ly.a, Ly.c, Ly.b, Ly.d, Rq.a, Rq.c, Rq.b, Rq.d, Gy.a, Gy.c, Gy.b, Gy.d);
-        const W4 Gl = shfl_up4(Gy);
-
-        if (out_col) {
+        // The row's arithmetic, with the divisions of a policy: the x-face
+        // i+1/2 from rows i .. i+2, the y-faces of row i (face j+1/2, normal v,
+        // transverse u; the left face from the left neighbour), the update of
+        // every lane's cell of row i and, in stage 2, its wave speeds.
+        struct RowOut {
+            W4 W2, S1, Fc, s;
+            double sx, sy, pc;
+        };
+        auto row = [&](auto& dp, auto& dv) {
+            RowOut o;
+            o.W2 = prim_d(dp, ring_row(i + 2), gm1);
+            o.S1 = limit4(Wq, Wq1, o.W2, lim);
+            const W4 M1 = half_back(Wq1, o.S1);
+            hlle4_d(dv, gamma, gm1, Pq.a, Pq.b, Pq.c, Pq.d, M1.a, M1.b, M1.c, M1.d, o.Fc.a, o.Fc.b, o.Fc.c, o.Fc.d);
+            const W4 sy = limit4(shfl_up4(Wq), Wq, shfl_dn4(Wq), lim);
+            const W4 Rq = shfl_dn4(half_back(Wq, sy));
+            const W4 Ly = half_step(Wq, sy, 0.5);
+            W4 Gy;
+            hlle4_d(dv, gamma, gm1, Ly.a, Ly.c, Ly.b, Ly.d, Rq.a, Rq.c, Rq.b, Rq.d, Gy.a, Gy.c, Gy.b, Gy.d);
+            const W4 Gl = shfl_up4(Gy);
             const W4 C0 = ring_row(i);
-            double s0 = C0.a - (dtdx * (Fc.a - Fm.a) + dtdy * (Gy.a - Gl.a));
-            double s1 = C0.b - (dtdx * (Fc.b - Fm.b) + dtdy * (Gy.b - Gl.b));
-            double s2 = C0.c - (dtdx * (Fc.c - Fm.c) + dtdy * (Gy.c - Gl.c));
-            double s3 = C0.d - (dtdx * (Fc.d - Fm.d) + dtdy * (Gy.d - Gl.d));
+            o.s.a = C0.a - (dtdx * (o.Fc.a - Fm.a) + dtdy * (Gy.a - Gl.a));
+            o.s.b = C0.b - (dtdx * (o.Fc.b - Fm.b) + dtdy * (Gy.b - Gl.b));
+            o.s.c = C0.c - (dtdx * (o.Fc.c - Fm.c) + dtdy * (Gy.c - Gl.c));
+            o.s.d = C0.d - (dtdx * (o.Fc.d - Fm.d) + dtdy * (Gy.d - Gl.d));
             if (STAGE == 2) {
                 const W4 N0 = ring_un(i);
-                s0 = 0.5 * (N0.a + s0);
-                s1 = 0.5 * (N0.b + s1);
-                s2 = 0.5 * (N0.c + s2);
-                s3 = 0.5 * (N0.d + s3);
-                double sx, syv;
-                const double pc = cell_speeds_p<double>(s0, s1, s2, s3, gamma, gm1, sx, syv);
+                o.s.a = 0.5 * (N0.a + o.s.a);
+                o.s.b = 0.5 * (N0.b + o.s.b);
+                o.s.c = 0.5 * (N0.c + o.s.c);
+                o.s.d = 0.5 * (N0.d + o.s.d);
+                o.pc = speeds_d(dv, o.s.a, o.s.b, o.s.c, o.s.d, gamma, gm1, o.sx, o.sy);
+            }
+            return o;
+        };
+        // The checked divisions first; if one of them that can reach an
+        // output could not be shown to be correctly rounded, the whole row
+        // again with IEEE divisions.  Either way the stored values are those
+        // of the IEEE arithmetic.  What reaches an output: the primitives of
+        // every lane up to the last ghost column (y-slopes of the lanes two
+        // away), and the fluxes and wave speeds of lanes 1..29 inside the
+        // domain (lane j-1's y-face is lane j's left face); lanes past the
+        // ghost columns read the row padding.
+        DivChecked dp, dc;
+        RowOut o = row(dp, dc);
+        const bool need = (!dp.ok && j <= ny + 1) || (!dc.ok && lane >= 1 && lane < 30 && j < ny);
+        if (__any_sync(0xffffffffu, need)) {
+            DivIeee di;
+            o = row(di, di);
+        }
+
+        if (out_col) {
+            const double s0 = o.s.a, s1 = o.s.b, s2 = o.s.c, s3 = o.s.d;
+            if (STAGE == 2) {
+                const double pc = o.pc;
                 if (!(s0 >= 1e-10) || !(pc > 0.0)) {
                     double pe = pc;
                     if (s0 > 0.0 && s0 < 1e-10) pe = gm1 * (s3 - ke2(s0, s1 / s0, s2 / s0));
                     if (!(s0 > 0.0) || !(pe > 0.0) || !(pe == pe))
                         flag_cell(a.ctrl, a.ctrl->step[a.p] + 1, s0, pe, i, j);
                 }
-                smx = smax(smx, sx);
-                smy = smax(smy, syv);
+                smx = smax(smx, o.sx);
+                smy = smax(smy, o.sy);
                 if (TOT) { t0 += s0; t1 += s1; t2 += s2; t3 += s3; }
             }
-            const long long o = g.at(i, j);
-            Uo[o] = s0; Uo[vs + o] = s1; Uo[2 * vs + o] = s2; Uo[3 * vs + o] = s3;
+            const long long oo = g.at(i, j);
+            Uo[oo] = s0; Uo[vs + oo] = s1; Uo[2 * vs + oo] = s2; Uo[3 * vs + oo] = s3;
             if (edge_col || i < 2 || i >= nx - 2) {
                 store_ghosts(Uo, g, 0, i, j, s0);
                 store_ghosts(Uo, g, 1, i, j, s1);
@@ -210,10 +298,10 @@ __device__ __forceinline__ void f64r_body(const StageArgs<double>& a, int strip,
                 store_ghosts(Uo, g, 3, i, j, s3);
             }
         }
-        Fm = Fc;
-        Pq = half_step(Wq1, S1, 0.5);
+        Fm = o.Fc;
+        Pq = half_step(Wq1, o.S1, 0.5);
         Wq = Wq1;
-        Wq1 = W2;
+        Wq1 = o.W2;
     }
     // no copy may land in shared memory after the warp has left
     cpd_wait<0>();
@@ -280,4 +368,26 @@ cudaError_t launch_2d_step_f64r(double* U, double* U1, const Geo2D& g, const Loo
     return cudaGetLastError();
 }
 
+namespace {
+__global__ void k_div_selftest(const double* a, const double* b, double* q, int* ok, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        bool k = true;
+        q[t] = div_rn_checked(a[t], b[t], k);
+        ok[t] = k ? 1 : 0;
+    }
+}
+}  // namespace
+
 }  // namespace nestb
+
+extern "C" nest_status nest_selftest_div_f64(const double* d_a, const double* d_b, double* d_q, int* d_ok, int n) {
+    if (!d_a || !d_b || !d_q || !d_ok || n < 0) return nestb::record_error(NEST_ERR_INVALID, "null array or n < 0");
+    if (n == 0) return NEST_OK;
+    nestb::k_div_selftest<<<(n + 255) / 256, 256>>>(d_a, d_b, d_q, d_ok, n);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess)
+        return nestb::record_error(NEST_ERR_CUDA, std::string("division self-test: ") + cudaGetErrorString(e));
+    return NEST_OK;
+}
