@@ -22,13 +22,15 @@
 // [2^-959, 2^961).  There ulp(q)/2 >= 2^-1012 and the threshold
 // |b| ulp(q)/2 ~ |a| 2^-53 are normal, nothing overflows, and a - b q is a
 // multiple of ulp(b) ulp(q) >= 2^-1074 smaller than 2^53 of them, so the
-// fused multiply-add forms it exactly.  Where |q| is a power of two the spacing below it is
-// half the spacing above, and the test takes the narrower interval on that
-// side.  a = 0 with b in that range gives the signed zero the IEEE division
-// gives.  Everything else, and any q the test does not accept, clears
-// `ok`; the caller then recomputes with the IEEE division.  (Scaling
-// numerators under 2^-959 by a power of two to keep them on the fast path
-// measured slower than recomputing the few rows that meet them.)
+// fused multiply-add forms it exactly.  Where |q| is a power of two the
+// spacing below it is half the spacing above, and the test takes the
+// narrower interval on both sides (such quotients are rare unless exact).
+// r = 0 is an exact quotient; with a = 0 and b finite and nonzero that is
+// the zero of sign(a) xor sign(b), the sign every quotient is given.
+// Everything else, and any q the test does not accept, clears `ok`; the
+// caller then recomputes with the IEEE division.  (Scaling numerators under
+// 2^-959 by a power of two to keep them on the fast path measured slower than
+// recomputing the few rows that meet them.)
 #pragma once
 
 #include <cuda_runtime.h>
@@ -46,23 +48,25 @@ __device__ __forceinline__ double div_rn_checked(double a, double b, bool& ok) {
     y = fma(y, fma(-b, y, 1.0), y);
     y = fma(y, fma(-b, y, 1.0), y);
     const double q0 = a * y;
-    const double q = fma(fma(-b, q0, a), y, q0);
+    const double qm = fma(fma(-b, q0, a), y, q0);
+    const int ha = __double2hiint(a), hb = __double2hiint(b);
+    // the IEEE quotient's sign is sign(a) xor sign(b); setting it also gives
+    // a zero quotient its sign
+    const double q = __hiloint2double((__double2hiint(qm) & 0x7fffffff) | ((ha ^ hb) & (int)0x80000000u),
+                                      __double2loint(qm));
     const double r = fma(-b, q, a);
     const int hq = __double2hiint(q);
     const unsigned exq = ((unsigned)hq >> 20) & 0x7ffu;
     // ulp(q)/2 = 2^(e(q) - 53): q's exponent field lowered by 53, mantissa 0
     const double hu = __hiloint2double((int)((unsigned)hq & 0x7ff00000u) - (53 << 20), 0);
-    // |q| a power of two: toward zero the spacing is ulp(q)/2, so a quotient
-    // below |q| must lie within ulp(q)/4 (a/b lies toward zero from q exactly
-    // when r and a differ in sign; r = 0 is an exact quotient)
+    // |q| a power of two: the spacing below it is half, so the narrower
+    // interval is used on both sides there
     const bool pow2 = (((unsigned)hq & 0xfffffu) | (unsigned)__double2loint(q)) == 0u;
-    const bool down = pow2 && ((__double2hiint(r) ^ __double2hiint(a)) < 0);
-    const double thr = fabs(b) * (down ? 0.5 * hu : hu);
-    const bool good = f64_exp_safe(f64_biased_exp(a)) && f64_exp_safe(exq) && fabs(r) < thr;
-    // a = 0: the IEEE quotient is zero with the sign of a xor the sign of b
-    const bool zero = a == 0.0 && f64_exp_safe(f64_biased_exp(b));
-    ok = ok && (good || zero);
-    return zero ? __hiloint2double((__double2hiint(a) ^ __double2hiint(b)) & (int)0x80000000u, 0) : q;
+    const double thr = fabs(b) * (pow2 ? 0.5 * hu : hu);
+    const bool aok = f64_exp_safe(f64_biased_exp(a));
+    // r = 0: an exact quotient (a = 0 included, b finite and nonzero: else r is NaN)
+    ok = ok && ((aok && f64_exp_safe(exq) && fabs(r) < thr) || (r == 0.0 && (aok || a == 0.0)));
+    return q;
 }
 
 }  // namespace nestb
