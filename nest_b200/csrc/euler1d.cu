@@ -60,7 +60,9 @@ __device__ __forceinline__ void ghost_copies_1d(double* A, int nt, int n, int h,
 // (examples/benchmark/benchmark_euler1d.cpp:113-209); primitives of a ghost
 // cell are the primitives of its source cell, which is what nest computes
 // from the copied conserved values.
-template <int K, int MAXT>
+// LIM (both resident kernels): the slope limiter fixed at compile time
+// (LIM_MINMOD, nest's default) or -1 to read it from the loop parameters.
+template <int K, int MAXT, int LIM>
 __global__ void __launch_bounds__(MAXT)
 k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int bc, LoopParams lp, StepCtrl* ctrl,
              int p) {
@@ -121,8 +123,8 @@ k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     const double* w = W + k * nt;
-                    sa[k] = limit(w[a] - w[a - 1], w[b] - w[a], lp.lim);
-                    sb[k] = limit(w[b] - w[a], w[b + 1] - w[b], lp.lim);
+                    sa[k] = limit(w[a] - w[a - 1], w[b] - w[a], LIM >= 0 ? LIM : lp.lim);
+                    sb[k] = limit(w[b] - w[a], w[b + 1] - w[b], LIM >= 0 ? LIM : lp.lim);
                 }
                 const double rL = W[a] + 0.5 * sa[0], uL = W[nt + a] + 0.5 * sa[1], pL = W[2 * nt + a] + 0.5 * sa[2];
                 const double rR = W[b] - 0.5 * sb[0], uR = W[nt + b] - 0.5 * sb[1], pR = W[2 * nt + b] - 0.5 * sb[2];
@@ -225,6 +227,7 @@ k1d_resident(double* __restrict__ Ug, int n, int h, double dx, double gamma, int
 // all CTAs derive the same dt.  The per-face and per-cell arithmetic is the
 // single-CTA kernel's (nest's OpenMP loop), so the result is the same bit for
 // bit; spreading the FP64 division / square-root work over NC SMs is the gain.
+template <int LIM>
 __global__ void __launch_bounds__(256)
 k1d_cluster(double* __restrict__ Ug, int n, int h, int m, double dx, double gamma, int bc, LoopParams lp,
             StepCtrl* ctrl, int p) {
@@ -311,8 +314,8 @@ k1d_cluster(double* __restrict__ Ug, int n, int h, int m, double dx, double gamm
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 const double* w = Wc + k * mw;
-                sa[k] = limit(w[a] - w[a - 1], w[bb] - w[a], lp.lim);
-                sb[k] = limit(w[bb] - w[a], w[bb + 1] - w[bb], lp.lim);
+                sa[k] = limit(w[a] - w[a - 1], w[bb] - w[a], LIM >= 0 ? LIM : lp.lim);
+                sb[k] = limit(w[bb] - w[a], w[bb + 1] - w[bb], LIM >= 0 ? LIM : lp.lim);
             }
             const double rL = Wc[a] + 0.5 * sa[0], uL = Wc[mw + a] + 0.5 * sa[1], pL = Wc[2 * mw + a] + 0.5 * sa[2];
             const double rR = Wc[bb] - 0.5 * sb[0], uR = Wc[mw + bb] - 0.5 * sb[1], pR = Wc[2 * mw + bb] - 0.5 * sb[2];
@@ -436,10 +439,11 @@ static cudaError_t launch_1d_cluster(double* U, int n, int h, double dx, double 
     const int threads = (m + 1 + 31) / 32 * 32;
     if (threads > 256) return cudaErrorNotSupported;
     const size_t smem = sizeof(double) * (size_t)(3 * m + 3 * m + 6 * (m + 4) + 3 * (m + 1) + 32);
+    auto kern = lp.lim == LIM_MINMOD ? k1d_cluster<LIM_MINMOD> : k1d_cluster<-1>;
     cudaError_t e;
-    if (NC > 8 && (e = cudaFuncSetAttribute(k1d_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
+    if (NC > 8 && (e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
         return e;
-    if ((e = cudaFuncSetAttribute(k1d_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+    if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
         return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(NC, 1, 1);
@@ -454,12 +458,12 @@ static cudaError_t launch_1d_cluster(double* U, int n, int h, double dx, double 
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int clusters = 0;
-    if ((e = cudaOccupancyMaxActiveClusters(&clusters, k1d_cluster, &cfg)) != cudaSuccess) {
+    if ((e = cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg)) != cudaSuccess) {
         cudaGetLastError();
         return cudaErrorNotSupported;
     }
     if (clusters < 1) return cudaErrorNotSupported;
-    return cudaLaunchKernelEx(&cfg, k1d_cluster, U, n, h, m, dx, gamma, bc, lp, ctrl, p);
+    return cudaLaunchKernelEx(&cfg, kern, U, n, h, m, dx, gamma, bc, lp, ctrl, p);
 }
 
 // Whether launch_1d_cluster can place a cluster of 16 or 8 CTAs for n cells
@@ -481,11 +485,13 @@ bool cluster_1d_available(int n, int h) {
         const int threads = (m + 1 + 31) / 32 * 32;
         if (threads > 256) continue;
         const size_t smem = sizeof(double) * (size_t)(3 * m + 3 * m + 6 * (m + 4) + 3 * (m + 1) + 32);
-        if (NC > 8 && cudaFuncSetAttribute(k1d_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        // both limiter instances use the same threads and shared memory; the
+        // minmod one stands for both
+        if (NC > 8 && cudaFuncSetAttribute(k1d_cluster<LIM_MINMOD>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
             cudaGetLastError();
             continue;
         }
-        if (cudaFuncSetAttribute(k1d_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        if (cudaFuncSetAttribute(k1d_cluster<LIM_MINMOD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
             cudaGetLastError();
             continue;
         }
@@ -501,7 +507,7 @@ bool cluster_1d_available(int n, int h) {
         cfg.attrs = at;
         cfg.numAttrs = 1;
         int clusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&clusters, k1d_cluster, &cfg) != cudaSuccess) {
+        if (cudaOccupancyMaxActiveClusters(&clusters, k1d_cluster<LIM_MINMOD>, &cfg) != cudaSuccess) {
             cudaGetLastError();
             continue;
         }
@@ -533,9 +539,10 @@ cudaError_t launch_1d_resident(double* U, int n, int h, double dx, double gamma,
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e == cudaSuccess) kern<<<1, threads, smem, st>>>(U, n, h, dx, gamma, bc, lp, ctrl, p);
     };
-    if (K == 2 && threads <= 640) go(k1d_resident<2, 640>);
-    else if (K == 2) go(k1d_resident<2, 1024>);
-    else go(k1d_resident<3, 1024>);
+    const bool mm = lp.lim == LIM_MINMOD;
+    if (K == 2 && threads <= 640) mm ? go(k1d_resident<2, 640, LIM_MINMOD>) : go(k1d_resident<2, 640, -1>);
+    else if (K == 2) mm ? go(k1d_resident<2, 1024, LIM_MINMOD>) : go(k1d_resident<2, 1024, -1>);
+    else mm ? go(k1d_resident<3, 1024, LIM_MINMOD>) : go(k1d_resident<3, 1024, -1>);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
