@@ -236,9 +236,10 @@ nest_status reverse_binomial(nest_adjoint* a, int l, int r, int k, int free, int
 }
 
 // Uniform schedule, one segment of L steps starting from seg_un[0]:
-// recompute (stage 1 into seg_u1[r], stage 2 out of place into seg_un[r+1],
-// dts read from seg_dts by step count) then reverse, lambda entering in
-// lam[0] and leaving in lam[0].  Captured once per L and replayed.
+// recompute (each step out of place into seg_un[r+1] with its U1 kept in
+// seg_u1[r] -- one launch in 1D -- and U1 alone for the last step; dts read
+// from seg_dts by step count) then reverse, lambda entering in lam[0] and
+// leaving in lam[0].  Captured once per L and replayed.
 nest_status segment_graph(nest_adjoint* a, int L, cudaGraphExec_t* out) {
     auto it = a->seg_graphs.find(L);
     if (it != a->seg_graphs.end()) { *out = it->second; return NEST_OK; }

@@ -102,7 +102,8 @@ nest_status nestb::rt::prepare(nest_solver* s) {
     return NEST_OK;
 }
 
-// Enqueue one step (two kernels) with parity p; `which` selects the stages.
+// Enqueue one step (the two stage kernels, in place) with parity p; `which`
+// selects the stages.
 cudaError_t nestb::rt::enqueue_step(nest_solver* s, const LoopParams& lp, int p, int which) {
     if (s->d.dim == 1 && s->d.precision == NEST_F32)
         return launch_1d_step_f32((float*)s->U, (float*)s->U1, s->d.nx, s->h, s->d.dx, s->d.gamma, s->d.bc_x, lp,

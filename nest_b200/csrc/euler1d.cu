@@ -10,11 +10,12 @@
 //     complete time loop (dt, ghost fill, both stages, Heun average) with no
 //     kernel boundary and no host round-trip per step.  Used while
 //     12 * (n + 4) doubles fit in shared memory.
-//   * tiled: stage kernels over 256-cell tiles; stage 2 fuses the Heun
-//     average, the ghost fill of the new state and the max-wave-speed
-//     reduction; dt is derived on the device from that maximum, so a step is
-//     two launches and no host synchronisation (steps are captured in CUDA
-//     graphs by the host code).
+//   * tiled (euler1d_tiled.cuh): a whole step per launch over 224-cell tiles
+//     (the stage-1 halo recomputed per CTA), or the two stage kernels; stage
+//     2 fuses the Heun average, the ghost fill of the new state and the
+//     max-wave-speed reduction; dt is derived on the device from that
+//     maximum, so steps need no host synchronisation (they are captured in
+//     CUDA graphs by the host code).
 #include <cooperative_groups.h>
 
 #include <map>
