@@ -16,7 +16,7 @@ from pathlib import Path
 import numpy as np
 
 CACHE = Path(os.environ.get("NEST_B200_TUNING", Path(__file__).resolve().parent / "tuning_cache.json"))
-ROWS = (16, 32, 64, 128)
+ROWS = (16, 24, 32, 64, 128)
 WARPS = (1, 2, 4, 8)
 DEFAULT = {"f32": (32, 4), "f64": (32, 4)}
 
