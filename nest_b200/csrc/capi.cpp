@@ -294,10 +294,10 @@ nest_status nest_solver_create(const nest_solver_desc* d, nest_solver** out) {
     s->h = d->halo;
     s->esize = d->precision == NEST_F64 ? 8 : 4;
     // default 2D launch shape: the autotuner's choice at 4096^2, one warp per
-    // block, 16-row tiles in FP32 and 24-row tiles in FP64 (whose tile
-    // prologue divides with IEEE division: 200 steps of the 4096^2 Riemann
-    // problem 2.313 -> 2.258 ms per step, 1000 steps of the 2048^2 KH state
-    // 585 -> 573 ms, against 16 rows; 32 rows took 626 ms on KH).  At 2048^2
+    // block, 16-row tiles in FP32 and 24-row tiles in FP64 (200 steps of the
+    // 4096^2 Riemann problem 2.269 -> 2.233 ms per step, 1000 steps of the
+    // 2048^2 KH state 585 -> 574 ms, against 16 rows; 32 rows took 627 ms on
+    // KH).  At 2048^2
     // the earlier default of 64-row tiles and 4 warps per block left half the
     // warp slots empty: a 4000-step FP32 KH forward took 891 ms against 540 ms.
     if (d->dim == 2) {

@@ -121,7 +121,6 @@ __device__ __forceinline__ void f64r_body(const StageArgs<double>& a, int strip,
     const int lane = threadIdx.x & 31;
     const double gamma = g.gamma;
     const double gm1 = g.gamma - 1.0;
-    const double igm1 = 1.0 / (g.gamma - 1.0);
 
     double dt;
     if (STAGE == 1) {
@@ -188,7 +187,6 @@ __device__ __forceinline__ void f64r_body(const StageArgs<double>& a, int strip,
         const long long o = g.at(i, min(j, ny + 1));
         return { __ldg(Ui + o), __ldg(Ui + vs + o), __ldg(Ui + 2 * vs + o), __ldg(Ui + 3 * vs + o) };
     };
-    auto prim = [&](const W4& c) -> W4 { return prim_win(cons2prim<double, false>(c.a, c.b, c.c, c.d, gm1)); };
 
     // prologue: rows i0-2 .. i0+1, the x-flux of face i0-1/2 and the upper
     // x-face state of row i0
@@ -201,13 +199,23 @@ __device__ __forceinline__ void f64r_body(const StageArgs<double>& a, int strip,
         cpd_commit();
         cpd_wait<0>();
         __syncwarp();
-        const W4 Wa = prim(c0), Wb = prim(c1);
-        Wq = prim(ring_row(i0));
-        Wq1 = prim(ring_row(i0 + 1));
-        const W4 Sb = limit4(Wa, Wb, Wq, lim), Sq = limit4(Wb, Wq, Wq1, lim);
-        const W4 L = half_step(Wb, Sb, 0.5), R = half_back(Wq, Sq);
-        hlle4<double>(gamma, gm1, igm1, L.a, L.b, L.c, L.d, R.a, R.b, R.c, R.d, Fm.a, Fm.b, Fm.c, Fm.d);
-        Pq = half_step(Wq, Sq, 0.5);
+        // with the checked divisions, again with IEEE ones if a lane up to the
+        // last ghost column failed one (as in the row loop below)
+        auto pro = [&](auto& d) {
+            const W4 Wa = prim_d(d, c0, gm1), Wb = prim_d(d, c1, gm1);
+            Wq = prim_d(d, ring_row(i0), gm1);
+            Wq1 = prim_d(d, ring_row(i0 + 1), gm1);
+            const W4 Sb = limit4(Wa, Wb, Wq, lim), Sq = limit4(Wb, Wq, Wq1, lim);
+            const W4 L = half_step(Wb, Sb, 0.5), R = half_back(Wq, Sq);
+            hlle4_d(d, gamma, gm1, L.a, L.b, L.c, L.d, R.a, R.b, R.c, R.d, Fm.a, Fm.b, Fm.c, Fm.d);
+            Pq = half_step(Wq, Sq, 0.5);
+        };
+        DivChecked dpro;
+        pro(dpro);
+        if (__any_sync(0xffffffffu, !dpro.ok && j <= ny + 1)) {
+            DivIeee di;
+            pro(di);
+        }
     }
 
     double smx = 0.0, smy = 0.0;
