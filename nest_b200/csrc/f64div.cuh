@@ -24,7 +24,10 @@
 // multiple of ulp(b) ulp(q) >= 2^-1074 smaller than 2^53 of them, so the
 // fused multiply-add forms it exactly.  Where |q| is a power of two the
 // spacing below it is half the spacing above, and the test takes the
-// narrower interval on both sides (such quotients are rare unless exact).
+// narrower interval on both sides.  That refuses nothing correct: a quotient
+// of two doubles is a power of two p or at least half the spacing above p
+// away from it, so a correct power-of-two quotient is exact (r = 0), and the
+// full-width test would be as sound there.
 // r = 0 is an exact quotient; with a = 0 and b finite and nonzero that is
 // the zero of sign(a) xor sign(b), the sign every quotient is given.
 // Everything else, and any q the test does not accept, clears `ok`; the
