@@ -53,3 +53,41 @@ def test_invalid_arguments_rejected_without_gpu():
     assert A.lib.nest_solver_step(None, 1, 0.4) == 1
     assert "null" in A.last_error()
     assert A.lib.nest_version() >= 10000
+
+
+def test_dropin_abi_refuses_bad_input_without_gpu():
+    """nest's euler1d_gpu_* entry points bound the way a nest maintainer would
+    bind them (a ctypes stub of its own, not the package's wrapper): bad sizes,
+    spacing, gamma or halo give NULL and a message instead of nest's C++
+    exception through extern "C" (src/backend_cuda/euler1d_solver.cu:24-29),
+    and every call on a null handle is refused without touching the device."""
+    import nest_b200
+    lib = C.CDLL(str(nest_b200.LIB_PATH))
+    vp, dp = C.c_void_p, C.POINTER(C.c_double)
+    lib.euler1d_gpu_create.restype, lib.euler1d_gpu_create.argtypes = vp, [C.c_int, C.c_int, C.c_double, C.c_double]
+    lib.euler1d_gpu_destroy.restype, lib.euler1d_gpu_destroy.argtypes = None, [vp]
+    lib.euler1d_gpu_upload.restype, lib.euler1d_gpu_upload.argtypes = None, [vp, dp]
+    lib.euler1d_gpu_download.restype, lib.euler1d_gpu_download.argtypes = None, [vp, dp]
+    lib.euler1d_gpu_compute_dt.restype, lib.euler1d_gpu_compute_dt.argtypes = C.c_double, [vp, C.c_double]
+    lib.euler1d_gpu_rk2_step.restype, lib.euler1d_gpu_rk2_step.argtypes = None, [vp, C.c_double]
+    lib.euler1d_gpu_run.restype, lib.euler1d_gpu_run.argtypes = C.c_int, [vp, C.c_double, C.c_double]
+    lib.euler1d_gpu_run_timed.restype = C.c_double
+    lib.euler1d_gpu_run_timed.argtypes = [vp, C.c_double, C.c_double, C.POINTER(C.c_int)]
+    lib.euler1d_gpu_status.restype, lib.euler1d_gpu_status.argtypes = C.c_int, [vp]
+    lib.nest_last_error.restype = C.c_char_p
+    invalid = 1  # NEST_ERR_INVALID
+    for args, words in [((0, 2, 0.1, 1.4), "interior"), ((-8, 2, 0.1, 1.4), "interior"),
+                        ((16, 1, 1 / 16, 1.4), "halo"), ((16, 2, 0.0, 1.4), "cell sizes"),
+                        ((16, 2, float("nan"), 1.4), "cell sizes"), ((16, 2, 1 / 16, 1.0), "gamma")]:
+        assert lib.euler1d_gpu_create(*args) is None, args
+        assert words in lib.nest_last_error().decode(), (args, lib.nest_last_error())
+    lib.euler1d_gpu_destroy(None)
+    lib.euler1d_gpu_upload(None, None)
+    lib.euler1d_gpu_download(None, None)
+    lib.euler1d_gpu_rk2_step(None, 1e-3)
+    assert lib.euler1d_gpu_compute_dt(None, 0.4) == 0.0
+    assert lib.euler1d_gpu_run(None, 0.2, 0.4) == -1
+    n = C.c_int(7)
+    assert lib.euler1d_gpu_run_timed(None, 0.2, 0.4, C.byref(n)) == -1.0
+    assert lib.euler1d_gpu_status(None) == invalid
+    assert "null" in lib.nest_last_error().decode()
