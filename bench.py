@@ -82,6 +82,8 @@ def parse():
     return ap.parse_args()
 
 
+L2_MB = 126  # B200 L2 cache, MB
+
 FORM_TEXT = {"f32": "FP32 state and arithmetic; FP64 conserved totals every step, FP64 time and dt, FP64 "
                      "positivity repair",
              "f32plain": "FP32 state and arithmetic; FP64 time and dt",
@@ -90,13 +92,15 @@ FORM_TEXT = {"f32": "FP32 state and arithmetic; FP64 conserved totals every step
 
 def workload_config(n: int, ws: int, head: str, slab: bool) -> dict:
     """`config` of the JSON line, the same keys for both arms."""
+    mb = 4 * (n + 4) ** 2 * (4 if head.startswith("f32") else 8) / 1e6
     return {"workload": f"riemann2d {ws * n}x{n} {head}", "nx": ws * n, "ny": n, "form": FORM_TEXT[head],
             "patches": f"{n // 256}x{n // 256} of 256^2" if n % 256 == 0 else "one",
             "bc": "outflow", "cfl": 0.4, "gamma": 1.4,
             "parallelism": "one GPU" if ws == 1 and not slab else
             f"{ws} x-slabs of {n}x{n} (NCCL halo rows + wave-speed all-reduce)",
-            "l2": "inputs larger than L2 (two state buffers of %.0f MB each)" % (
-                4 * (n + 4) ** 2 * (4 if head.startswith("f32") else 8) / 1e6)}
+            "l2": ("inputs larger than L2 (two state buffers of %.0f MB each)" if mb > L2_MB else
+                   "inputs fit in L2 (two state buffers of %.1f MB each): a small case, not the benchmark "
+                   "workload") % mb}
 
 
 def load_problems():
