@@ -53,7 +53,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["riemann2d"], default="riemann2d")
-    ap.add_argument("--n", type=int, default=4096, help="cells per axis")
+    ap.add_argument("--n", "--size", dest="n", type=int, default=4096,
+                    help="cells per axis (--size under torchrun, whose parser takes --n for its own options)")
     ap.add_argument("--forms", default="f64,f32,f32plain",
                     help="forms to time (f64: the plain FP64 form; f32: FP32 with FP64 totals and repair; "
                          "f32plain: FP32 without them); the first is the headline")
@@ -952,37 +953,41 @@ def cpu_baseline(n: int, budget_s: float, steps: int, final_f64=None):
 
 
 def run_reference(args, rank):
-    """CPU arm: each step is one RK2 step of a sample of the workload -- the
-    first nx_s rows of the n x n grid as an outflow domain -- sized from the
-    warm-up timing so the whole run stays within minutes."""
+    """CPU arm: each step is one RK2 step of a sample of the workload the CUDA
+    arm runs at this world size -- the first nx_s rows of the (N n) x n grid
+    (N = world size) as an outflow domain -- sized from a one-step probe so
+    the whole run stays within minutes."""
     from oracle.oracle import BC_OUTFLOW, Oracle
     riemann_2d = load_problems().riemann_2d
     orc = Oracle()
     th = host_threads()
     orc.set_threads(th)
+    ws = max(1, int(os.environ.get("WORLD_SIZE", args.gpus)))
     n = args.n
-    nx_s = n
-    U = np.ascontiguousarray(riemann_2d(n, n))
+    nxg = ws * n
+    dx, dy = 1 / nxg, 1 / n
+    nx_s = min(nxg, n)
+    U = np.ascontiguousarray(riemann_2d(nxg, n, rows=(0, nx_s)))
     t0 = time.perf_counter()
-    orc.run2d(U, n, n, 2, 1 / n, 1 / n, 1.4, 0.4, nsteps=1, bc=BC_OUTFLOW)
+    orc.run2d(U, nx_s, n, 2, dx, dy, 1.4, 0.4, nsteps=1, bc=BC_OUTFLOW)
     t1 = time.perf_counter() - t0
     per_step_budget = 90.0 / max(1, args.steps + args.warmup)
     if t1 > per_step_budget:
-        nx_s = max(64, int(n * per_step_budget / t1) // 64 * 64)
-    Us = np.ascontiguousarray(riemann_2d(n, n)[:, : nx_s + 4, :])
-    orc.run2d(Us, nx_s, n, 2, 1 / n, 1 / n, 1.4, 0.4, nsteps=max(1, args.warmup), bc=BC_OUTFLOW)
-    Us = np.ascontiguousarray(riemann_2d(n, n)[:, : nx_s + 4, :])
+        nx_s = max(64, int(nx_s * per_step_budget / t1) // 64 * 64)
+    Us = np.ascontiguousarray(riemann_2d(nxg, n, rows=(0, nx_s)))
+    orc.run2d(Us, nx_s, n, 2, dx, dy, 1.4, 0.4, nsteps=max(1, args.warmup), bc=BC_OUTFLOW)
+    Us = np.ascontiguousarray(riemann_2d(nxg, n, rows=(0, nx_s)))
     t0 = time.perf_counter()
-    orc.run2d(Us, nx_s, n, 2, 1 / n, 1 / n, 1.4, 0.4, nsteps=args.steps, bc=BC_OUTFLOW)
+    orc.run2d(Us, nx_s, n, 2, dx, dy, 1.4, 0.4, nsteps=args.steps, bc=BC_OUTFLOW)
     el = time.perf_counter() - t0
     value = nx_s * n * 2 * args.steps / el
-    sample = (f"{args.steps} RK2 steps of a {nx_s}x{n} slab of the {n}x{n} FP64 diagonal Riemann problem, "
+    sample = (f"{args.steps} RK2 steps of a {nx_s}x{n} slab of the {nxg}x{n} FP64 diagonal Riemann problem, "
               f"oracle/euler_oracle.c (the scheme's CPU restatement; nest has no 2D RK2), OpenMP {th} threads")
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(n, 1, "f64", False),
+        "config": workload_config(n, ws, "f64", False),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": th, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

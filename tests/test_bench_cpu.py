@@ -41,3 +41,22 @@ def test_reference_arm_json_line():
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     loaded = [l for l in out.stdout.splitlines() if l.startswith("LOADED")]
     assert loaded == ["LOADED []"], loaded
+
+
+def test_reference_arm_under_torchrun():
+    """Launched like the CUDA arm at N = 2 (torchrun, one process per rank):
+    rank 0 alone prints one line, for the same (2 n) x n workload the CUDA arm
+    runs at that world size; the other rank exits 0 without work."""
+    import random
+    port = random.randint(29100, 29900)
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl", "reference",
+           "--gpus", "2", "--size", "256", "--steps", "2", "--warmup", "1"]
+    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, out.stdout[-2000:]
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["config"]["workload"] == "riemann2d 512x256 f64" and d["config"]["nx"] == 512
+    assert "512x256" in d["cpu_baseline"]["sample"]
