@@ -355,6 +355,10 @@ nest_status nest_selftest_div_f64(const double* d_a, const double* d_b, double* 
 /* Every call looks up the array's address in the current device's context  */
 /* and waits for its stream (it reads the step count back every 32 steps).  */
 /* All calls share the array: calls that overlap on the GPU race.           */
+/* The array reaches device memory with the library's code module, which    */
+/* CUDA loads into a context on first use (with the default lazy module     */
+/* loading, at the first call of this function there): a caller that must   */
+/* not allocate after start-up makes its first call during start-up.        */
 /*                                                                          */
 /* d_state: device SoA [var * n_total + i], n_total = n_interior + 2 n_halo */
 /* (nest's layout), advanced in place from time 0 to t_final with CFL dt,   */

@@ -10,7 +10,10 @@
 // call itself never allocates or frees memory.
 //
 // The array is part of the library image: every GPU that loads the library
-// holds it (about 1.6 MB) until the process exits.  All calls share it, and it
+// holds it (about 1.6 MB) until the process exits.  It reaches device memory
+// when CUDA loads this file's code module into a context, which under the
+// default lazy module loading happens at the first call; a caller that must
+// not allocate after start-up makes its first call during start-up.  All calls share it, and it
 // keeps the previous call's contents; each call clears the control block it
 // needs, and calls that overlap on the GPU (two streams, or two threads at
 // once) race on it.
