@@ -261,7 +261,10 @@ nest_status segment_graph(nest_adjoint* a, int L, cudaGraphExec_t* out) {
         e = cudaMemcpyAsync(a->lam[0], a->lam[1], a->s->state_bytes(), cudaMemcpyDeviceToDevice, st);
     cudaGraph_t g;
     cudaError_t e2 = cudaStreamEndCapture(st, &g);
-    if (e != cudaSuccess) return cuda_fail(e, "segment capture");
+    if (e != cudaSuccess) {
+        if (e2 == cudaSuccess) cudaGraphDestroy(g);
+        return cuda_fail(e, "segment capture");
+    }
     if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
     cudaGraphExec_t ge;
     cudaError_t e3 = cudaGraphInstantiate(&ge, g, 0);

@@ -166,7 +166,10 @@ nest_status enqueue_steps(nest_solver* s, int nsteps, const LoopParams& lp) {
                 else
                     for (int i = 0; i < GRAPH_STEPS && e == cudaSuccess; ++i, p ^= 1) e = enqueue_step(s, lp, p);
                 cudaError_t e2 = cudaStreamEndCapture(s->st, &g);
-                if (e != cudaSuccess) return cuda_fail(e, "step capture");
+                if (e != cudaSuccess) {
+                    if (e2 == cudaSuccess) cudaGraphDestroy(g);
+                    return cuda_fail(e, "step capture");
+                }
                 if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
                 cudaGraphExec_t ge;
                 cudaError_t e3 = cudaGraphInstantiate(&ge, g, 0);
@@ -1020,7 +1023,10 @@ nest_status nest_batch_step(nest_batch* b, int nsteps, double cfl) {
                 cudaError_t e = cudaSuccess;
                 for (int i = 0; i < GRAPH_STEPS && e == cudaSuccess; ++i, p ^= 1) e = batch_enqueue_step(b, lp, p);
                 cudaError_t e2 = cudaStreamEndCapture(b->st, &g);
-                if (e != cudaSuccess) return cuda_fail(e, "batch capture");
+                if (e != cudaSuccess) {
+                    if (e2 == cudaSuccess) cudaGraphDestroy(g);
+                    return cuda_fail(e, "batch capture");
+                }
                 if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
                 cudaGraphExec_t ge;
                 cudaError_t e3 = cudaGraphInstantiate(&ge, g, 0);

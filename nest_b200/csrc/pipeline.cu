@@ -427,7 +427,10 @@ nest_status nest_pipeline_run(nest_pipeline* p, void* d_state, double t_final, i
         cudaError_t e = cudaSuccess;
         for (int k = 0; k < PIPE_GRAPH_STEPS && e == cudaSuccess; ++k) e = launch_all(p, d_state, st);
         cudaError_t e2 = cudaStreamEndCapture(st, &g);
-        if (e != cudaSuccess) return cuda_fail(e, "pipeline capture");
+        if (e != cudaSuccess) {
+            if (e2 == cudaSuccess) cudaGraphDestroy(g);
+            return cuda_fail(e, "pipeline capture");
+        }
         if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
         cudaGraphExec_t ge;
         cudaError_t e3 = cudaGraphInstantiate(&ge, g, 0);

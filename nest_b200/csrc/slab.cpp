@@ -247,7 +247,10 @@ nest_status nest_slab_step(nest_solver* s, nest_slab_comm* c, int lo, int hi, in
                 int p = s->parity;
                 for (int i = 0; i < GRAPH_STEPS && r == NEST_OK; ++i, p ^= 1) r = enqueue_slab_step(s, c, lo, hi, lp, p);
                 cudaError_t e2 = cudaStreamEndCapture(s->st, &g);
-                if (r != NEST_OK) return r;
+                if (r != NEST_OK) {
+                    if (e2 == cudaSuccess) cudaGraphDestroy(g);
+                    return r;
+                }
                 if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
                 cudaError_t e3 = cudaGraphInstantiate(&ge, g, 0);
                 cudaGraphDestroy(g);
