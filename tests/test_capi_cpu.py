@@ -45,6 +45,15 @@ def test_invalid_arguments_rejected_without_gpu():
         dict(dim=2, nx=8, ny=8, halo=3),
         dict(dim=1, nx=16, precision=A.F32, flags=A.FLAG_TOTALS),
         dict(dim=2, nx=8, ny=8, dx=-1.0),
+        dict(dim=2, nx=8, ny=8, dy=float("nan")),
+        dict(dim=2, nx=65536, ny=32769),                       # more than 2^31 cells
+        dict(dim=2, nx=8, ny=8, precision=7),
+        dict(dim=2, nx=8, ny=8, bc=(A.BC_OUTFLOW, 5)),
+        dict(dim=1, nx=16, bc=(5, 5)),
+        dict(dim=1, nx=16, flags=A.FLAG_SPLIT_COMPAT),         # nest's split sweeps are 2D FP64
+        dict(dim=2, nx=8, ny=8, precision=A.F32, flags=A.FLAG_SPLIT_COMPAT),
+        dict(dim=2, nx=8, ny=8, flags=A.FLAG_SPLIT_COMPAT | A.FLAG_TOTALS),
+        dict(dim=2, nx=8, ny=8, flags=A.FLAG_LIMITER_MC | A.FLAG_LIMITER_NONE),
     ]
     for kw in bad:
         with pytest.raises(nb.NestError) as e:
