@@ -100,3 +100,36 @@ def test_dropin_abi_refuses_bad_input_without_gpu():
     assert lib.euler1d_gpu_run_timed(None, 0.2, 0.4, C.byref(n)) == -1.0
     assert lib.euler1d_gpu_status(None) == invalid
     assert "null" in lib.nest_last_error().decode()
+
+
+def test_other_constructors_reject_bad_input_without_gpu():
+    """Batches, nest's patch exchange plans and device pipelines check their
+    arguments on the host before any device call (so these run without a
+    GPU): nest's exchange needs every patch to hold at least `halo` interior
+    cells per axis (its halo copies read that far into the neighbour)."""
+    import nest_b200 as nb
+    from nest_b200 import _capi as A
+    from nest_b200.batch import Batch
+    from nest_b200.exchange import PeriodicExchange
+    from nest_b200.pipeline import Pipeline
+    for kw in [dict(nx=[], ny=[]), dict(nx=[64, 2], ny=[64, 64]), dict(nx=[64], ny=[64], gamma=1.0),
+               dict(nx=[64], ny=[64], bc=(A.BC_PERIODIC, 5)), dict(nx=[64], ny=[64], precision=7)]:
+        with pytest.raises(nb.NestError) as e:
+            Batch(**kw)
+        assert e.value.status == A.NEST_ERR_INVALID, kw
+    with pytest.raises(nb.NestError) as e:
+        Batch([64], [64], flags=A.FLAG_LIMITER_MC)
+    assert e.value.status == A.NEST_ERR_UNSUPPORTED
+    for kw in [dict(dim=3, nx=64, npx=2, nvars=3, halo=2), dict(dim=1, nx=64, npx=2, nvars=0, halo=2),
+               dict(dim=1, nx=64, npx=2, nvars=3, halo=0), dict(dim=1, nx=3, npx=2, nvars=3, halo=2),
+               dict(dim=2, nx=64, npx=2, nvars=4, halo=2, ny=64, npy=0),
+               dict(dim=2, nx=64, npx=2, nvars=4, halo=2, ny=5, npy=3)]:
+        with pytest.raises(nb.NestError) as e:
+            PeriodicExchange(**kw)
+        assert e.value.status == A.NEST_ERR_INVALID, kw
+    for kw in [dict(dim=3, nx=64, npx=2), dict(dim=1, nx=64, npx=2, dx=-1.0), dict(dim=1, nx=64, npx=2, gamma=1.0),
+               dict(dim=1, nx=64, npx=2, nwork=17), dict(dim=1, nx=64, npx=2, limiter=9),
+               dict(dim=1, nx=3, npx=2)]:
+        with pytest.raises(nb.NestError) as e:
+            Pipeline(**kw)
+        assert e.value.status == A.NEST_ERR_INVALID, kw
